@@ -1,0 +1,160 @@
+/*
+ * iqcp.h -- C ABI of libiqcp_gpu.so, the B200 (sm_100a) direct Fock-build and
+ * two-electron nuclear-gradient engine for Cartesian Gaussian basis sets.
+ *
+ * The entry points replace, one for one, the reference's (ExaPsi/IQCP,
+ * crates/qc-core) Rust functions on this path; each declaration names the
+ * function it stands in for.  Plain pointers and sizes only.
+ *
+ * Conventions
+ *  - Matrices are nbf x nbf, row-major, FP64.  All matrices on this path are
+ *    symmetric, so row- and column-major (the reference's nalgebra DMatrix is
+ *    column-major) hold the same elements.
+ *  - The density carries the RHF factor 2 (D = 2 C_occ C_occ^T), as in
+ *    scf/mod.rs:780-794.
+ *  - Basis functions are Cartesian, shell by shell in the order given, with
+ *    components ordered xx,xy,xz,yy,yz,zz for d (integrals/cartesian.rs:113).
+ *    Every primitive x component carries coef * N(alpha, i, j, k)
+ *    (integrals/overlap.rs:343); the caller passes the raw tabulated
+ *    contraction coefficients.
+ *  - Every function returns IQCP_OK (0) or a negative status; the message of
+ *    the last failure on a context is available from iqcp_last_error().
+ *  - Calls on one context are synchronous with respect to the host and not
+ *    thread-safe; use one context per host thread.
+ */
+#ifndef IQCP_H_
+#define IQCP_H_
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum iqcp_status {
+  IQCP_OK = 0,
+  IQCP_ERR_ARG = -1,        /* invalid argument (sizes, unsupported L, NULL) */
+  IQCP_ERR_CUDA = -2,       /* a CUDA runtime call failed */
+  IQCP_ERR_NOMEM = -3,      /* device or host allocation failed */
+  IQCP_ERR_NUMERIC = -4,    /* non-finite input or result */
+  IQCP_ERR_NODEVICE = -5,   /* no usable sm_100 device */
+  IQCP_ERR_BASIS = -6       /* unknown basis name or element */
+};
+
+enum iqcp_precision {
+  IQCP_FP64 = 0,            /* all quadrature in FP64 */
+  IQCP_MIXED = 1            /* FP32 quadrature for weak quartets, FP64 roots and accumulation */
+};
+
+/* A basis as qc-core's BasisSet holds it (basis/mod.rs:113-130). */
+typedef struct iqcp_basis_desc {
+  int n_shells;
+  int n_atoms;
+  const int* l;               /* [n_shells] angular momentum, 0..2 */
+  const int* nprim;           /* [n_shells] primitives per shell */
+  const int* atom_of_shell;   /* [n_shells] */
+  const double* center;       /* [3*n_shells] bohr */
+  const double* exps;         /* [sum nprim] exponents, shell by shell */
+  const double* coefs;        /* [sum nprim] raw contraction coefficients */
+  const double* atom_xyz;     /* [3*n_atoms] bohr */
+  const int* z;               /* [n_atoms] atomic numbers */
+} iqcp_basis_desc;
+
+typedef struct iqcp_options {
+  double schwarz_threshold;   /* 1e-12: eri/mod.rs:1258 SCHWARZ_THRESHOLD */
+  double prim_threshold;      /* 1e-15: K_ij and K_ij*K_kl screens, eri/mod.rs:603,611 */
+  int precision;              /* enum iqcp_precision */
+  double mixed_cutoff;        /* MIXED: quartets with Q_ij*Q_kl*max|D| below this use FP32 */
+  int device;                 /* CUDA device ordinal */
+} iqcp_options;
+
+typedef struct iqcp_ctx iqcp_ctx;
+
+/* Default options (thresholds of the reference, FP64). */
+void iqcp_default_options(iqcp_options* opts);
+
+/*
+ * Build a basis for atoms (bohr) from the built-in tables.
+ * Replaces BasisSet::build (basis/mod.rs:164) with get_element_basis
+ * (basis/builtin.rs:97).  Call once with the array pointers NULL to get the
+ * counts, then again with arrays of those sizes.  Returns IQCP_ERR_BASIS for an
+ * unknown basis name or an element outside H..Ar.
+ */
+int iqcp_basis_build(const char* basis_name, int n_atoms, const int* z, const double* xyz,
+                     int* n_shells, int* n_prims, int* nbf, int* l, int* nprim,
+                     int* atom_of_shell, double* center, double* exps, double* coefs);
+
+/*
+ * Create a context for one basis (geometry): uploads the basis, builds the
+ * class-sorted shell-pair data and the Schwarz bounds on the device and the
+ * screened quartet lists.  Stands in for the set-up half of eri_compressed
+ * (integrals/eri/mod.rs:992-1030, compute_schwarz_bounds :1263).
+ */
+int iqcp_create(const iqcp_basis_desc* basis, const iqcp_options* opts, iqcp_ctx** out);
+void iqcp_destroy(iqcp_ctx* ctx);
+const char* iqcp_last_error(const iqcp_ctx* ctx);
+int iqcp_nbf(const iqcp_ctx* ctx);
+
+/* Run the context's work on this CUDA stream (cudaStream_t); NULL = its own stream. */
+int iqcp_set_stream(iqcp_ctx* ctx, void* stream);
+
+/*
+ * Coulomb and exchange matrices from a density, host buffers.
+ * J_mn = sum_ls D_ls (mn|ls),  K_mn = sum_ls D_ls (ml|ns).
+ * Replaces build_jk / build_coulomb / build_exchange (dft/ks_scf.rs:1306,1342,1369).
+ * K may be NULL (Coulomb only).
+ */
+int iqcp_jk(iqcp_ctx* ctx, const double* D, double* J, double* K);
+
+/*
+ * Fock matrix F = H + J - 1/2 * k_scale * K, host buffers.  k_scale = 1 is RHF
+ * (build_fock, scf/mod.rs:825-881); k_scale = hf_frac is the hybrid KS form
+ * (dft/ks_scf.rs:1795-1843, 1953-1960).
+ */
+int iqcp_fock(iqcp_ctx* ctx, const double* H, const double* D, double k_scale, double* F);
+
+/* Device-pointer forms of iqcp_jk / iqcp_fock for data resident in HBM. */
+int iqcp_jk_device(iqcp_ctx* ctx, const double* d_D, double* d_J, double* d_K);
+int iqcp_fock_device(iqcp_ctx* ctx, const double* d_H, const double* d_D, double k_scale,
+                     double* d_F);
+
+/*
+ * Two-electron part of the nuclear gradient, host buffers:
+ * grad[3*atom + dir] += sum over unique quartets of w * d(ij|kl)/dR with
+ * w = sum_perm [1/2 D_ij D_kl - 1/4 hf_frac D_ik D_jl].
+ * Replaces eri_gradient_fused (scf/gradient.rs:1430-1566) with
+ * compute_symmetry_weight (:1570-1640) and shell_eri_with_derivatives
+ * (integrals/eri/mod.rs:2035-2548).
+ */
+int iqcp_eri_grad(iqcp_ctx* ctx, const double* D, double hf_frac, double* grad);
+int iqcp_eri_grad_device(iqcp_ctx* ctx, const double* d_D, double hf_frac, double* d_grad);
+
+/*
+ * All unique ERIs in the reference's 8-fold compressed layout,
+ * idx = P(P+1)/2 + Q, P = pair(i,j) >= Q = pair(k,l), pair(i,j) = i(i+1)/2 + j.
+ * Replaces eri_compressed (integrals/eri/mod.rs:992-1070); out holds
+ * n_pairs(n_pairs+1)/2 doubles, n_pairs = nbf(nbf+1)/2.  Small bases only.
+ */
+int iqcp_eri_compressed(iqcp_ctx* ctx, double* out, long long out_len);
+
+/* Schwarz bounds Q[n_shells*n_shells] (compute_schwarz_bounds, eri/mod.rs:1263). */
+int iqcp_schwarz(iqcp_ctx* ctx, double* Q);
+
+/*
+ * Batched Boys function F_0..F_m_max(T) and Rys roots (t^2) / weights on the
+ * device, host buffers; the device forms of boys_eval_all (boys/mod.rs:327)
+ * and rys_roots (rys/mod.rs:253).  F is [n][m_max+1], roots/weights [n][nroots].
+ */
+int iqcp_boys_batch(int m_max, int n, const double* T, double* F);
+int iqcp_rys_batch(int nroots, int n, const double* T, double* roots, double* weights);
+
+/*
+ * Counters of the last J/K or gradient call: [0] screened shell quartets,
+ * [1] kernel launches, [2] device time of the quartet kernels in microseconds
+ * (CUDA events on the context stream), [3] quartets evaluated in FP32.
+ */
+int iqcp_last_stats(const iqcp_ctx* ctx, double* stats4);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* IQCP_H_ */

@@ -1,0 +1,313 @@
+"""iqcp_b200: B200-native direct Fock build and two-electron gradient.
+
+Thin ctypes binding of ``libiqcp_gpu.so`` (C ABI in ``include/iqcp.h``).  The
+names mirror the reference's qc-core entry points on this path:
+
+=============================  ==================================================
+here                           reference (ExaPsi/IQCP crates/qc-core)
+=============================  ==================================================
+``BasisSet.build``             ``BasisSet::build`` (basis/mod.rs:164)
+``FockEngine.build_jk``        ``build_jk`` (dft/ks_scf.rs:1369)
+``FockEngine.build_fock``      ``build_fock`` (scf/mod.rs:825)
+``FockEngine.eri_gradient``    ``eri_gradient_fused`` (scf/gradient.rs:1430)
+``FockEngine.eri_compressed``  ``eri_compressed`` (integrals/eri/mod.rs:992)
+``FockEngine.schwarz``         ``compute_schwarz_bounds`` (eri/mod.rs:1263)
+``boys_eval_all``              ``boys_eval_all`` (boys/mod.rs:327), batched
+``rys_roots``                  ``rys_roots`` (rys/mod.rs:253), batched
+=============================  ==================================================
+
+There is no CPU fallback: every compute call goes to the CUDA library and
+raises ``IqcpError`` when the library or a B200 is missing.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+__all__ = ["BasisSet", "FockEngine", "IqcpError", "boys_eval_all", "rys_roots", "lib_path",
+           "load_library", "ANGSTROM_TO_BOHR", "FP64", "MIXED"]
+
+ANGSTROM_TO_BOHR = 1.8897261245650618  # constants.rs:63
+FP64, MIXED = 0, 1
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+_c_int_p = ctypes.POINTER(ctypes.c_int)
+_c_dbl_p = ctypes.POINTER(ctypes.c_double)
+
+STATUS = {0: "ok", -1: "invalid argument", -2: "CUDA error", -3: "out of memory",
+          -4: "non-finite value", -5: "no usable sm_100 device", -6: "unknown basis or element"}
+
+
+class IqcpError(RuntimeError):
+    """A libiqcp_gpu call returned a non-zero status."""
+
+    def __init__(self, code, msg=""):
+        self.code = code
+        super().__init__("iqcp status %d (%s)%s" % (code, STATUS.get(code, "?"), (": " + msg) if msg else ""))
+
+
+class _BasisDesc(ctypes.Structure):
+    _fields_ = [("n_shells", ctypes.c_int), ("n_atoms", ctypes.c_int),
+                ("l", _c_int_p), ("nprim", _c_int_p), ("atom_of_shell", _c_int_p),
+                ("center", _c_dbl_p), ("exps", _c_dbl_p), ("coefs", _c_dbl_p),
+                ("atom_xyz", _c_dbl_p), ("z", _c_int_p)]
+
+
+class _Options(ctypes.Structure):
+    _fields_ = [("schwarz_threshold", ctypes.c_double), ("prim_threshold", ctypes.c_double),
+                ("precision", ctypes.c_int), ("mixed_cutoff", ctypes.c_double), ("device", ctypes.c_int)]
+
+
+def lib_path():
+    return os.path.join(_HERE, "libiqcp_gpu.so")
+
+
+EXPORTS = {
+    "iqcp_default_options": (None, [ctypes.POINTER(_Options)]),
+    "iqcp_basis_build": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, _c_int_p, _c_dbl_p, _c_int_p, _c_int_p,
+                                        _c_int_p, _c_int_p, _c_int_p, _c_int_p, _c_dbl_p, _c_dbl_p, _c_dbl_p]),
+    "iqcp_create": (ctypes.c_int, [ctypes.POINTER(_BasisDesc), ctypes.POINTER(_Options),
+                                   ctypes.POINTER(ctypes.c_void_p)]),
+    "iqcp_destroy": (None, [ctypes.c_void_p]),
+    "iqcp_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
+    "iqcp_nbf": (ctypes.c_int, [ctypes.c_void_p]),
+    "iqcp_set_stream": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "iqcp_jk": (ctypes.c_int, [ctypes.c_void_p, _c_dbl_p, _c_dbl_p, _c_dbl_p]),
+    "iqcp_fock": (ctypes.c_int, [ctypes.c_void_p, _c_dbl_p, _c_dbl_p, ctypes.c_double, _c_dbl_p]),
+    "iqcp_jk_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "iqcp_fock_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double,
+                                        ctypes.c_void_p]),
+    "iqcp_eri_grad": (ctypes.c_int, [ctypes.c_void_p, _c_dbl_p, ctypes.c_double, _c_dbl_p]),
+    "iqcp_eri_grad_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double, ctypes.c_void_p]),
+    "iqcp_eri_compressed": (ctypes.c_int, [ctypes.c_void_p, _c_dbl_p, ctypes.c_longlong]),
+    "iqcp_schwarz": (ctypes.c_int, [ctypes.c_void_p, _c_dbl_p]),
+    "iqcp_boys_batch": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _c_dbl_p, _c_dbl_p]),
+    "iqcp_rys_batch": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _c_dbl_p, _c_dbl_p, _c_dbl_p]),
+    "iqcp_last_stats": (ctypes.c_int, [ctypes.c_void_p, _c_dbl_p]),
+}
+
+
+def load_library():
+    """Load libiqcp_gpu.so from the package directory (raises if it is missing)."""
+    global _LIB
+    if _LIB is None:
+        path = lib_path()
+        if not os.path.exists(path):
+            raise IqcpError(-5, "libiqcp_gpu.so not built (run __graft_entry__.build())")
+        lib = ctypes.CDLL(path)
+        for name, (res, args) in EXPORTS.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _LIB = lib
+    return _LIB
+
+
+def _dp(a):
+    return a.ctypes.data_as(_c_dbl_p)
+
+
+def _ip(a):
+    return a.ctypes.data_as(_c_int_p)
+
+
+class BasisSet:
+    """Cartesian Gaussian basis for a molecule, in qc-core's shell order."""
+
+    def __init__(self, name, z, xyz, l, nprim, atom_of_shell, center, exps, coefs):
+        self.name = name
+        self.z = np.ascontiguousarray(z, dtype=np.int32)
+        self.xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+        self.l = np.ascontiguousarray(l, dtype=np.int32)
+        self.nprim = np.ascontiguousarray(nprim, dtype=np.int32)
+        self.atom_of_shell = np.ascontiguousarray(atom_of_shell, dtype=np.int32)
+        self.center = np.ascontiguousarray(center, dtype=np.float64).reshape(-1, 3)
+        self.exps = np.ascontiguousarray(exps, dtype=np.float64)
+        self.coefs = np.ascontiguousarray(coefs, dtype=np.float64)
+        ncart = (self.l + 1) * (self.l + 2) // 2
+        self.offsets = np.concatenate([[0], np.cumsum(ncart)[:-1]]).astype(np.int32)
+        self.n_basis = int(ncart.sum())
+        self.n_electrons = int(self.z.sum())
+
+    @property
+    def n_shells(self):
+        return len(self.l)
+
+    @property
+    def n_atoms(self):
+        return len(self.z)
+
+    @classmethod
+    def build(cls, atoms, basis_name):
+        """atoms: list of (Z, (x, y, z) in bohr) -- BasisSet::build (basis/mod.rs:164)."""
+        lib = load_library()
+        z = np.array([a[0] for a in atoms], dtype=np.int32)
+        xyz = np.array([a[1] for a in atoms], dtype=np.float64).reshape(-1, 3)
+        ns, npr, nb = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        name = basis_name.encode()
+        rc = lib.iqcp_basis_build(name, len(z), _ip(z), _dp(xyz), ctypes.byref(ns), ctypes.byref(npr),
+                                  ctypes.byref(nb), None, None, None, None, None, None)
+        if rc:
+            raise IqcpError(rc, "basis %r" % basis_name)
+        l = np.zeros(ns.value, np.int32)
+        nprim = np.zeros(ns.value, np.int32)
+        aos = np.zeros(ns.value, np.int32)
+        center = np.zeros((ns.value, 3))
+        exps = np.zeros(npr.value)
+        coefs = np.zeros(npr.value)
+        rc = lib.iqcp_basis_build(name, len(z), _ip(z), _dp(xyz), ctypes.byref(ns), ctypes.byref(npr),
+                                  ctypes.byref(nb), _ip(l), _ip(nprim), _ip(aos), _dp(center), _dp(exps),
+                                  _dp(coefs))
+        if rc:
+            raise IqcpError(rc)
+        return cls(basis_name.lower(), z, xyz, l, nprim, aos, center, exps, coefs)
+
+    def nuclear_repulsion(self):
+        e = 0.0
+        for i in range(self.n_atoms):
+            for j in range(i):
+                e += self.z[i] * self.z[j] / np.linalg.norm(self.xyz[i] - self.xyz[j])
+        return float(e)
+
+    def as_args(self):
+        """Plain arrays in the C ABI's shell layout (also used by the oracle)."""
+        return (self.n_shells, self.l, self.nprim, self.atom_of_shell, self.center, self.exps, self.coefs,
+                self.n_atoms, self.xyz, self.z)
+
+    def _desc(self):
+        d = _BasisDesc()
+        d.n_shells, d.n_atoms = self.n_shells, self.n_atoms
+        d.l, d.nprim, d.atom_of_shell = _ip(self.l), _ip(self.nprim), _ip(self.atom_of_shell)
+        d.center, d.exps, d.coefs = _dp(self.center), _dp(self.exps), _dp(self.coefs)
+        d.atom_xyz, d.z = _dp(self.xyz), _ip(self.z)
+        return d
+
+
+class FockEngine:
+    """A per-geometry context of libiqcp_gpu (iqcp_create ... iqcp_destroy)."""
+
+    def __init__(self, basis, precision=FP64, schwarz_threshold=1e-12, prim_threshold=1e-15,
+                 mixed_cutoff=1e-9, device=0):
+        lib = load_library()
+        self._lib = lib
+        self.basis = basis
+        opts = _Options()
+        lib.iqcp_default_options(ctypes.byref(opts))
+        opts.schwarz_threshold = schwarz_threshold
+        opts.prim_threshold = prim_threshold
+        opts.precision = precision
+        opts.mixed_cutoff = mixed_cutoff
+        opts.device = device
+        self._desc = basis._desc()
+        h = ctypes.c_void_p()
+        rc = lib.iqcp_create(ctypes.byref(self._desc), ctypes.byref(opts), ctypes.byref(h))
+        self._h = h
+        if rc:
+            msg = lib.iqcp_last_error(h).decode() if h.value else ""
+            self.close()
+            raise IqcpError(rc, msg)
+        self.nbf = lib.iqcp_nbf(h)
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self._lib.iqcp_destroy(self._h)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, rc):
+        if rc:
+            raise IqcpError(rc, self._lib.iqcp_last_error(self._h).decode())
+
+    def _mat(self, a):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        if a.shape != (self.nbf, self.nbf):
+            raise ValueError("expected a %dx%d matrix" % (self.nbf, self.nbf))
+        return a
+
+    def build_jk(self, D, with_k=True):
+        D = self._mat(D)
+        J = np.empty_like(D)
+        K = np.empty_like(D) if with_k else None
+        self._check(self._lib.iqcp_jk(self._h, _dp(D), _dp(J), _dp(K) if with_k else None))
+        return (J, K) if with_k else J
+
+    def build_fock(self, H, D, k_scale=1.0):
+        H, D = self._mat(H), self._mat(D)
+        F = np.empty_like(D)
+        self._check(self._lib.iqcp_fock(self._h, _dp(H), _dp(D), float(k_scale), _dp(F)))
+        return F
+
+    def eri_gradient(self, D, hf_frac=1.0):
+        D = self._mat(D)
+        g = np.zeros((self.basis.n_atoms, 3))
+        self._check(self._lib.iqcp_eri_grad(self._h, _dp(D), float(hf_frac), _dp(g)))
+        return g
+
+    def eri_compressed(self):
+        n = self.nbf
+        npair = n * (n + 1) // 2
+        out = np.empty(npair * (npair + 1) // 2)
+        self._check(self._lib.iqcp_eri_compressed(self._h, _dp(out), out.size))
+        return out
+
+    def schwarz(self):
+        q = np.zeros((self.basis.n_shells, self.basis.n_shells))
+        self._check(self._lib.iqcp_schwarz(self._h, _dp(q)))
+        return q
+
+    def last_stats(self):
+        s = np.zeros(4)
+        self._check(self._lib.iqcp_last_stats(self._h, _dp(s)))
+        return {"quartets": int(s[0]), "launches": int(s[1]), "kernel_us": float(s[2]), "fp32_quartets": int(s[3])}
+
+    # device-resident forms (pointers to nbf*nbf doubles in HBM, e.g. torch tensors' data_ptr())
+    def jk_device(self, d_D, d_J, d_K=None):
+        self._check(self._lib.iqcp_jk_device(self._h, ctypes.c_void_p(d_D), ctypes.c_void_p(d_J),
+                                             ctypes.c_void_p(d_K) if d_K else None))
+
+    def fock_device(self, d_H, d_D, k_scale, d_F):
+        self._check(self._lib.iqcp_fock_device(self._h, ctypes.c_void_p(d_H), ctypes.c_void_p(d_D),
+                                               float(k_scale), ctypes.c_void_p(d_F)))
+
+    def eri_gradient_device(self, d_D, hf_frac, d_grad):
+        self._check(self._lib.iqcp_eri_grad_device(self._h, ctypes.c_void_p(d_D), float(hf_frac),
+                                                   ctypes.c_void_p(d_grad)))
+
+    def set_stream(self, stream_handle):
+        self._check(self._lib.iqcp_set_stream(self._h, ctypes.c_void_p(stream_handle)))
+
+
+def boys_eval_all(m_max, T):
+    """F_0..F_m_max at each T on the device: array [len(T), m_max+1]."""
+    lib = load_library()
+    T = np.ascontiguousarray(T, dtype=np.float64).ravel()
+    F = np.empty((T.size, m_max + 1))
+    rc = lib.iqcp_boys_batch(int(m_max), T.size, _dp(T), _dp(F))
+    if rc:
+        raise IqcpError(rc)
+    return F
+
+
+def rys_roots(nroots, T):
+    """Rys roots (t^2) and weights on the device: two arrays [len(T), nroots]."""
+    lib = load_library()
+    T = np.ascontiguousarray(T, dtype=np.float64).ravel()
+    R = np.empty((T.size, nroots))
+    W = np.empty((T.size, nroots))
+    rc = lib.iqcp_rys_batch(int(nroots), T.size, _dp(T), _dp(R), _dp(W))
+    if rc:
+        raise IqcpError(rc)
+    return R, W

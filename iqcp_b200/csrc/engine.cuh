@@ -1,0 +1,117 @@
+// Shared device/host definitions of the ERI engine: shell-pair tables in HBM,
+// quartet tasks, Cartesian component tables.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace iqcp {
+
+// Angular-momentum classes of a shell pair with la >= lb:
+// 0 ss, 1 ps, 2 pp, 3 ds, 4 dp, 5 dd  (index la*(la+1)/2 + lb)
+constexpr int kNumPairClasses = 6;
+constexpr int kMaxL = 2;
+
+__host__ __device__ constexpr int ncart(int l) { return (l + 1) * (l + 2) / 2; }
+__host__ __device__ constexpr int pair_class(int la, int lb) { return la * (la + 1) / 2 + lb; }
+__host__ __device__ constexpr int class_la(int c) { return c == 0 ? 0 : (c <= 2 ? 1 : 2); }
+__host__ __device__ constexpr int class_lb(int c) { return c - class_la(c) * (class_la(c) + 1) / 2; }
+
+// Cartesian powers, reference order (integrals/cartesian.rs:113-136):
+// x exponent descending, then y exponent descending.
+__host__ __device__ constexpr int cart_pow(int l, int c, int axis) {
+  // l = 0: (000); l = 1: x y z; l = 2: xx xy xz yy yz zz
+  return l == 0 ? 0
+       : l == 1 ? (c == axis ? 1 : 0)
+       : (axis == 0 ? (c == 0 ? 2 : (c <= 2 ? 1 : 0))
+          : axis == 1 ? (c == 1 ? 1 : (c == 3 ? 2 : (c == 4 ? 1 : 0)))
+                      : (c == 2 ? 1 : (c == 4 ? 1 : (c == 5 ? 2 : 0))));
+}
+
+// One primitive pair of a shell pair (A first, la >= lb), 64 bytes.
+struct __align__(16) PrimPair {
+  double p;       // alpha_a + alpha_b
+  double P[3];    // Gaussian product centre
+  double K;       // exp(-alpha_a alpha_b / p |AB|^2)  (screening value)
+  double cK;      // K * c_a * c_b * Nrad(alpha_a, la) * Nrad(alpha_b, lb)
+  double aa;      // alpha_a
+  double ab;      // alpha_b
+};
+
+// One shell pair (la >= lb after the swap), 64 bytes.
+struct __align__(16) ShellPair {
+  double A[3];
+  double B[3];
+  double Q;       // Schwarz bound sqrt(max |(ab|ab)|)
+  int pstart;     // first PrimPair
+  int np;         // number of PrimPairs (K >= prim threshold)
+  int oa, ob;     // first basis function of shell a / b
+  int sa, sb;     // shell indices (for same-shell degeneracy)
+  int atom_a, atom_b;
+  int comp;       // reference composite index si(si+1)/2+sj, si>=sj
+  int pad;
+};
+
+// Unit of work for one warp: one bra pair against up to 32 consecutive ket
+// pairs of a class list.
+struct QuartetTask {
+  int bra;        // ShellPair index
+  int ket0;       // first position in the ket class list
+  int nket;       // 1..32
+  int diag;       // 1 when bra and ket lists are the same class (position ket0+i == bra_pos => pair with itself)
+  int bra_pos;    // position of the bra in its class list
+  int flags;      // bit0: evaluate in FP32 (mixed precision)
+};
+
+// Kernel argument blocks (passed by value).
+struct JKArgs {
+  const ShellPair* pairs;
+  const PrimPair* pp;
+  const int* ket_list;
+  const QuartetTask* tasks;
+  int ntasks;
+  const double* D;   // angular-scaled density
+  int nbf;
+  double* J;         // unsymmetrised accumulators (nbf x nbf)
+  double* K;         // may be null
+  double prim_thr;
+};
+
+struct StoreArgs {
+  const ShellPair* pairs;
+  const PrimPair* pp;
+  const int* ket_list;
+  const QuartetTask* tasks;
+  int ntasks;
+  double* out;
+  double prim_thr;
+};
+
+struct GradArgs {
+  const ShellPair* pairs;
+  const PrimPair* pp;
+  const int* ket_list;
+  const QuartetTask* tasks;
+  int ntasks;
+  const double* D;   // angular-scaled density
+  int nbf;
+  double xscale;     // 0.25 * hf_frac
+  double* grad;      // natoms x 3
+  double prim_thr;
+  double schwarz_thr;
+};
+
+// Host launchers (eri_kernels.cu)
+cudaError_t launch_jk(int X, int Y, const JKArgs& a, cudaStream_t st);
+cudaError_t launch_store(int X, int Y, const StoreArgs& a, cudaStream_t st);
+cudaError_t launch_grad(int X, int Y, const GradArgs& a, cudaStream_t st);
+cudaError_t launch_schwarz(int X, ShellPair* pairs, const PrimPair* pp, const int* list, int n,
+                           double thr, cudaStream_t st);
+cudaError_t launch_scale_density(const double* D, const double* ang, int n, double* Ds, cudaStream_t st);
+cudaError_t launch_symmetrize(const double* X, const double* ang, int n, double* out, cudaStream_t st);
+cudaError_t launch_fock(const double* H, const double* Jt, const double* Kt, const double* ang, int n,
+                        double kscale, double* F, cudaStream_t st);
+cudaError_t launch_boys_batch(int m, int n, const double* T, double* F, cudaStream_t st);
+cudaError_t launch_rys_batch(int nr, int n, const double* T, double* R, double* W, cudaStream_t st);
+
+}  // namespace iqcp

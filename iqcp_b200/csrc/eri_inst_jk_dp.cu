@@ -1,0 +1,6 @@
+// Instantiation of the jk quartet kernels for bra class (dp|
+#include "eri_templates.cuh"
+
+namespace iqcp {
+template cudaError_t launch_jk_bra<2, 1>(int, const JKArgs&, cudaStream_t);
+}  // namespace iqcp

@@ -1,0 +1,6 @@
+// Instantiation of the store quartet kernels for bra class (dd|
+#include "eri_templates.cuh"
+
+namespace iqcp {
+template cudaError_t launch_store_bra<2, 2>(int, const StoreArgs&, cudaStream_t);
+}  // namespace iqcp

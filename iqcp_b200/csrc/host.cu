@@ -1,0 +1,583 @@
+// Host runtime of libiqcp_gpu.so: basis construction from the built-in
+// tables, per-geometry shell-pair tables and screened quartet work lists in
+// HBM, and the extern "C" entry points declared in include/iqcp.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/iqcp.h"
+#include "engine.cuh"
+
+#include "basis_tables.inc"
+
+using namespace iqcp;
+
+namespace {
+
+struct ClassList {
+  std::vector<int> pairs;   // ShellPair ids sorted by Q descending
+};
+
+struct TaskRange {
+  int X, Y;
+  int first, count;         // into the task array
+};
+
+}  // namespace
+
+struct iqcp_ctx {
+  std::string err;
+  int device = 0;
+  iqcp_options opt;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  int nbf = 0, n_shells = 0, n_atoms = 0;
+  std::vector<int> shell_l, shell_off, shell_atom;
+  // device tables
+  ShellPair* d_pairs = nullptr;
+  PrimPair* d_pp = nullptr;
+  int* d_ket_list = nullptr;      // class lists concatenated
+  QuartetTask* d_tasks = nullptr;
+  double* d_ang = nullptr;        // per basis function angular factor
+  double* d_Ds = nullptr;         // scaled density
+  double* d_Jt = nullptr;
+  double* d_Kt = nullptr;
+  double* d_io[4] = {nullptr, nullptr, nullptr, nullptr};  // staging for host-buffer calls
+  double* d_grad = nullptr;
+  // host copies
+  std::vector<ShellPair> pairs;
+  std::vector<int> list_offset;   // per class, into d_ket_list
+  std::vector<ClassList> classes;
+  std::vector<TaskRange> ranges;
+  long long n_quartets = 0;
+  double stats[4] = {0, 0, 0, 0};
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+namespace {
+
+int fail(iqcp_ctx* c, int code, const std::string& msg) {
+  if (c) c->err = msg;
+  return code;
+}
+
+#define CK(call)                                                                              \
+  do {                                                                                        \
+    cudaError_t e_ = (call);                                                                  \
+    if (e_ != cudaSuccess)                                                                    \
+      return fail(ctx, IQCP_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));    \
+  } while (0)
+
+double rad_norm(double a, int l) {
+  // (2a/pi)^{3/4} (4a)^{l/2}, the alpha-dependent part of overlap.rs:343
+  const double tap = 2.0 * a / M_PI;
+  double v = std::sqrt(std::sqrt(tap * tap * tap));
+  const double fa = 4.0 * a;
+  if (l == 1) v *= std::sqrt(fa);
+  else if (l == 2) v *= fa;
+  return v;
+}
+
+double ang_host(int l, int c) {
+  return (l == 2 && (c == 0 || c == 3 || c == 5)) ? 1.0 / std::sqrt(3.0) : 1.0;
+}
+
+int basis_id(const char* name) {
+  std::string s;
+  for (const char* p = name; *p; ++p) {
+    const char ch = (char)std::tolower((unsigned char)*p);
+    if (ch != ' ' && ch != '_') s.push_back(ch);
+  }
+  if (s == "sto-3g" || s == "sto3g") return 0;
+  if (s == "3-21g" || s == "321g") return 1;
+  if (s == "6-31g" || s == "631g") return 2;
+  if (s == "6-31g*" || s == "631g*" || s == "6-31gs" || s == "631gs" || s == "6-31g(d)" || s == "631g(d)") return 3;
+  if (s == "6-31+g*" || s == "631+g*" || s == "6-31+gs" || s == "631+gs" || s == "6-31+g(d)" || s == "631+g(d)") return 4;
+  if (s == "cc-pvdz" || s == "ccpvdz") return 5;
+  return -1;
+}
+
+// Build class lists and quartet tasks from Schwarz bounds held in ctx->pairs.
+void build_tasks(iqcp_ctx* ctx, std::vector<int>& ket_list, std::vector<QuartetTask>& tasks) {
+  const double thr = ctx->opt.schwarz_threshold;
+  ctx->classes.assign(kNumPairClasses, ClassList());
+  for (int i = 0; i < (int)ctx->pairs.size(); ++i) {
+    const ShellPair& p = ctx->pairs[i];
+    const int cls = pair_class(ctx->shell_l[p.sa], ctx->shell_l[p.sb]);
+    ctx->classes[cls].pairs.push_back(i);
+  }
+  ctx->list_offset.assign(kNumPairClasses + 1, 0);
+  ket_list.clear();
+  for (int c = 0; c < kNumPairClasses; ++c) {
+    auto& v = ctx->classes[c].pairs;
+    std::stable_sort(v.begin(), v.end(), [&](int a, int b) { return ctx->pairs[a].Q > ctx->pairs[b].Q; });
+    ctx->list_offset[c] = (int)ket_list.size();
+    ket_list.insert(ket_list.end(), v.begin(), v.end());
+  }
+  ctx->list_offset[kNumPairClasses] = (int)ket_list.size();
+  tasks.clear();
+  ctx->ranges.clear();
+  ctx->n_quartets = 0;
+  for (int X = 0; X < kNumPairClasses; ++X)
+    for (int Y = 0; Y <= X; ++Y) {
+      const auto& LX = ctx->classes[X].pairs;
+      const auto& LY = ctx->classes[Y].pairs;
+      TaskRange r{X, Y, (int)tasks.size(), 0};
+      for (int b = 0; b < (int)LX.size(); ++b) {
+        const double qb = ctx->pairs[LX[b]].Q;
+        // ket prefix with qb*qk >= thr (lists sorted by Q descending)
+        int lo = 0, hi = (int)LY.size();
+        while (lo < hi) {
+          const int mid = (lo + hi) / 2;
+          if (qb * ctx->pairs[LY[mid]].Q < thr) hi = mid; else lo = mid + 1;
+        }
+        int nk = lo;
+        if (X == Y) nk = std::min(nk, b + 1);
+        ctx->n_quartets += nk;
+        for (int k0 = 0; k0 < nk; k0 += 32) {
+          QuartetTask t;
+          t.bra = LX[b];
+          t.ket0 = ctx->list_offset[Y] + k0;
+          t.nket = std::min(32, nk - k0);
+          t.diag = (X == Y) ? 1 : 0;
+          t.bra_pos = ctx->list_offset[X] + b;
+          t.flags = 0;
+          tasks.push_back(t);
+        }
+      }
+      r.count = (int)tasks.size() - r.first;
+      ctx->ranges.push_back(r);
+    }
+}
+
+int ensure_device(iqcp_ctx* ctx) {
+  CK(cudaSetDevice(ctx->device));
+  return IQCP_OK;
+}
+
+int run_jk_device(iqcp_ctx* ctx, const double* dD, bool want_k) {
+  const int n = ctx->nbf;
+  const size_t bytes = sizeof(double) * (size_t)n * n;
+  CK(launch_scale_density(dD, ctx->d_ang, n, ctx->d_Ds, ctx->stream));
+  CK(cudaMemsetAsync(ctx->d_Jt, 0, bytes, ctx->stream));
+  if (want_k) CK(cudaMemsetAsync(ctx->d_Kt, 0, bytes, ctx->stream));
+  CK(cudaEventRecord(ctx->ev0, ctx->stream));
+  int launches = 0;
+  for (const TaskRange& r : ctx->ranges) {
+    if (r.count == 0) continue;
+    JKArgs a;
+    a.pairs = ctx->d_pairs;
+    a.pp = ctx->d_pp;
+    a.ket_list = ctx->d_ket_list;
+    a.tasks = ctx->d_tasks + r.first;
+    a.ntasks = r.count;
+    a.D = ctx->d_Ds;
+    a.nbf = n;
+    a.J = ctx->d_Jt;
+    a.K = want_k ? ctx->d_Kt : nullptr;
+    a.prim_thr = ctx->opt.prim_threshold;
+    CK(launch_jk(r.X, r.Y, a, ctx->stream));
+    ++launches;
+  }
+  CK(cudaEventRecord(ctx->ev1, ctx->stream));
+  ctx->stats[0] = (double)ctx->n_quartets;
+  ctx->stats[1] = launches;
+  return IQCP_OK;
+}
+
+int finish_stats(iqcp_ctx* ctx) {
+  float ms = 0.f;
+  CK(cudaEventSynchronize(ctx->ev1));
+  CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+  ctx->stats[2] = ms * 1e3;
+  return IQCP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void iqcp_default_options(iqcp_options* o) {
+  o->schwarz_threshold = 1e-12;
+  o->prim_threshold = 1e-15;
+  o->precision = IQCP_FP64;
+  o->mixed_cutoff = 1e-9;
+  o->device = 0;
+}
+
+int iqcp_basis_build(const char* basis_name, int n_atoms, const int* z, const double* xyz,
+                     int* n_shells, int* n_prims, int* nbf, int* l, int* nprim, int* atom_of_shell,
+                     double* center, double* exps, double* coefs) {
+  if (!basis_name || n_atoms <= 0 || !z || !xyz) return IQCP_ERR_ARG;
+  const int bid = basis_id(basis_name);
+  if (bid < 0) return IQCP_ERR_BASIS;
+  int ns = 0, np = 0, nb = 0;
+  for (int a = 0; a < n_atoms; ++a) {
+    if (z[a] < 1 || z[a] > 18) return IQCP_ERR_BASIS;
+    for (int r = 0; r < kNumShellRecords; ++r) {
+      const int* rec = kShellRecords[r];
+      if (rec[0] != bid || rec[1] != z[a]) continue;
+      if (l) {
+        l[ns] = rec[2];
+        nprim[ns] = rec[3];
+        atom_of_shell[ns] = a;
+        for (int d = 0; d < 3; ++d) center[3 * ns + d] = xyz[3 * a + d];
+        for (int k = 0; k < rec[3]; ++k) {
+          exps[np + k] = kPrimitives[rec[4] + k][0];
+          coefs[np + k] = kPrimitives[rec[4] + k][1];
+        }
+      }
+      ++ns;
+      np += rec[3];
+      nb += ncart(rec[2]);
+    }
+  }
+  if (n_shells) *n_shells = ns;
+  if (n_prims) *n_prims = np;
+  if (nbf) *nbf = nb;
+  return IQCP_OK;
+}
+
+const char* iqcp_last_error(const iqcp_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+int iqcp_nbf(const iqcp_ctx* ctx) { return ctx ? ctx->nbf : 0; }
+
+int iqcp_create(const iqcp_basis_desc* b, const iqcp_options* opts, iqcp_ctx** out) {
+  if (!b || !out || b->n_shells <= 0 || b->n_atoms <= 0) return IQCP_ERR_ARG;
+  iqcp_ctx* ctx = new iqcp_ctx();
+  *out = ctx;
+  if (opts) ctx->opt = *opts;
+  else iqcp_default_options(&ctx->opt);
+  ctx->device = ctx->opt.device;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= ctx->device)
+    return fail(ctx, IQCP_ERR_NODEVICE, "no CUDA device available");
+  cudaDeviceProp prop;
+  CK(cudaGetDeviceProperties(&prop, ctx->device));
+  if (prop.major != 10) return fail(ctx, IQCP_ERR_NODEVICE, "libiqcp_gpu is built for sm_100a only");
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking));
+  ctx->stream = ctx->own_stream;
+  CK(cudaEventCreate(&ctx->ev0));
+  CK(cudaEventCreate(&ctx->ev1));
+
+  ctx->n_shells = b->n_shells;
+  ctx->n_atoms = b->n_atoms;
+  std::vector<int> pstart(b->n_shells + 1, 0);
+  int off = 0;
+  for (int s = 0; s < b->n_shells; ++s) {
+    if (b->l[s] < 0 || b->l[s] > kMaxL) return fail(ctx, IQCP_ERR_ARG, "angular momentum above d");
+    if (b->nprim[s] <= 0) return fail(ctx, IQCP_ERR_ARG, "shell without primitives");
+    if (b->atom_of_shell[s] < 0 || b->atom_of_shell[s] >= b->n_atoms) return fail(ctx, IQCP_ERR_ARG, "bad atom index");
+    ctx->shell_l.push_back(b->l[s]);
+    ctx->shell_off.push_back(off);
+    ctx->shell_atom.push_back(b->atom_of_shell[s]);
+    off += ncart(b->l[s]);
+    pstart[s + 1] = pstart[s] + b->nprim[s];
+  }
+  ctx->nbf = off;
+  const double kthr = ctx->opt.prim_threshold;
+
+  // shell pairs si >= sj (reference order), A = higher-L shell
+  std::vector<PrimPair> pps;
+  for (int si = 0; si < b->n_shells; ++si)
+    for (int sj = 0; sj <= si; ++sj) {
+      int sa = si, sb = sj;
+      if (b->l[sj] > b->l[si]) std::swap(sa, sb);
+      ShellPair sp;
+      std::memset(&sp, 0, sizeof(sp));
+      for (int d = 0; d < 3; ++d) {
+        sp.A[d] = b->center[3 * sa + d];
+        sp.B[d] = b->center[3 * sb + d];
+      }
+      sp.sa = sa;
+      sp.sb = sb;
+      sp.oa = ctx->shell_off[sa];
+      sp.ob = ctx->shell_off[sb];
+      sp.atom_a = b->atom_of_shell[sa];
+      sp.atom_b = b->atom_of_shell[sb];
+      sp.comp = si * (si + 1) / 2 + sj;
+      sp.pstart = (int)pps.size();
+      double ab2 = 0;
+      for (int d = 0; d < 3; ++d) ab2 += (sp.A[d] - sp.B[d]) * (sp.A[d] - sp.B[d]);
+      for (int i = 0; i < b->nprim[sa]; ++i)
+        for (int j = 0; j < b->nprim[sb]; ++j) {
+          const double ea = b->exps[pstart[sa] + i], eb = b->exps[pstart[sb] + j];
+          const double K = std::exp(-(ea * eb / (ea + eb)) * ab2);
+          if (K < kthr) continue;
+          PrimPair q;
+          q.p = ea + eb;
+          for (int d = 0; d < 3; ++d) q.P[d] = (ea * sp.A[d] + eb * sp.B[d]) / q.p;
+          q.K = K;
+          q.cK = K * b->coefs[pstart[sa] + i] * rad_norm(ea, b->l[sa]) * b->coefs[pstart[sb] + j] *
+                 rad_norm(eb, b->l[sb]);
+          q.aa = ea;
+          q.ab = eb;
+          pps.push_back(q);
+        }
+      sp.np = (int)pps.size() - sp.pstart;
+      ctx->pairs.push_back(sp);
+    }
+  if (pps.empty()) pps.push_back(PrimPair());
+  const int npairs = (int)ctx->pairs.size();
+  CK(cudaMalloc(&ctx->d_pairs, sizeof(ShellPair) * npairs));
+  CK(cudaMalloc(&ctx->d_pp, sizeof(PrimPair) * pps.size()));
+  CK(cudaMemcpy(ctx->d_pairs, ctx->pairs.data(), sizeof(ShellPair) * npairs, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(ctx->d_pp, pps.data(), sizeof(PrimPair) * pps.size(), cudaMemcpyHostToDevice));
+
+  // Schwarz bounds on the device, one launch per pair class
+  {
+    std::vector<std::vector<int>> by_cls(kNumPairClasses);
+    for (int i = 0; i < npairs; ++i) {
+      const ShellPair& p = ctx->pairs[i];
+      by_cls[pair_class(ctx->shell_l[p.sa], ctx->shell_l[p.sb])].push_back(i);
+    }
+    int* d_list = nullptr;
+    CK(cudaMalloc(&d_list, sizeof(int) * npairs));
+    int pos = 0;
+    for (int c = 0; c < kNumPairClasses; ++c) {
+      if (by_cls[c].empty()) continue;
+      CK(cudaMemcpy(d_list + pos, by_cls[c].data(), sizeof(int) * by_cls[c].size(), cudaMemcpyHostToDevice));
+      CK(launch_schwarz(c, ctx->d_pairs, ctx->d_pp, d_list + pos, (int)by_cls[c].size(), kthr, ctx->stream));
+      pos += (int)by_cls[c].size();
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
+    CK(cudaFree(d_list));
+    CK(cudaMemcpy(ctx->pairs.data(), ctx->d_pairs, sizeof(ShellPair) * npairs, cudaMemcpyDeviceToHost));
+  }
+  std::vector<int> ket_list;
+  std::vector<QuartetTask> tasks;
+  build_tasks(ctx, ket_list, tasks);
+  if (ket_list.empty()) ket_list.push_back(0);
+  if (tasks.empty()) tasks.push_back(QuartetTask());
+  CK(cudaMalloc(&ctx->d_ket_list, sizeof(int) * ket_list.size()));
+  CK(cudaMemcpy(ctx->d_ket_list, ket_list.data(), sizeof(int) * ket_list.size(), cudaMemcpyHostToDevice));
+  CK(cudaMalloc(&ctx->d_tasks, sizeof(QuartetTask) * tasks.size()));
+  CK(cudaMemcpy(ctx->d_tasks, tasks.data(), sizeof(QuartetTask) * tasks.size(), cudaMemcpyHostToDevice));
+
+  std::vector<double> ang(ctx->nbf);
+  for (int s = 0; s < b->n_shells; ++s)
+    for (int c = 0; c < ncart(b->l[s]); ++c) ang[ctx->shell_off[s] + c] = ang_host(b->l[s], c);
+  const size_t nn = (size_t)ctx->nbf * ctx->nbf;
+  CK(cudaMalloc(&ctx->d_ang, sizeof(double) * ctx->nbf));
+  CK(cudaMemcpy(ctx->d_ang, ang.data(), sizeof(double) * ctx->nbf, cudaMemcpyHostToDevice));
+  CK(cudaMalloc(&ctx->d_Ds, sizeof(double) * nn));
+  CK(cudaMalloc(&ctx->d_Jt, sizeof(double) * nn));
+  CK(cudaMalloc(&ctx->d_Kt, sizeof(double) * nn));
+  for (int i = 0; i < 4; ++i) CK(cudaMalloc(&ctx->d_io[i], sizeof(double) * nn));
+  CK(cudaMalloc(&ctx->d_grad, sizeof(double) * 3 * ctx->n_atoms));
+  return IQCP_OK;
+}
+
+void iqcp_destroy(iqcp_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  cudaFree(ctx->d_pairs);
+  cudaFree(ctx->d_pp);
+  cudaFree(ctx->d_ket_list);
+  cudaFree(ctx->d_tasks);
+  cudaFree(ctx->d_ang);
+  cudaFree(ctx->d_Ds);
+  cudaFree(ctx->d_Jt);
+  cudaFree(ctx->d_Kt);
+  for (int i = 0; i < 4; ++i) cudaFree(ctx->d_io[i]);
+  cudaFree(ctx->d_grad);
+  if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+  if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+  if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+  delete ctx;
+}
+
+int iqcp_set_stream(iqcp_ctx* ctx, void* stream) {
+  if (!ctx) return IQCP_ERR_ARG;
+  ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
+  return IQCP_OK;
+}
+
+int iqcp_jk_device(iqcp_ctx* ctx, const double* dD, double* dJ, double* dK) {
+  if (!ctx || !dD || !dJ) return IQCP_ERR_ARG;
+  int rc = ensure_device(ctx);
+  if (rc) return rc;
+  rc = run_jk_device(ctx, dD, dK != nullptr);
+  if (rc) return rc;
+  CK(launch_symmetrize(ctx->d_Jt, ctx->d_ang, ctx->nbf, dJ, ctx->stream));
+  if (dK) CK(launch_symmetrize(ctx->d_Kt, ctx->d_ang, ctx->nbf, dK, ctx->stream));
+  return finish_stats(ctx);
+}
+
+int iqcp_fock_device(iqcp_ctx* ctx, const double* dH, const double* dD, double k_scale, double* dF) {
+  if (!ctx || !dH || !dD || !dF) return IQCP_ERR_ARG;
+  int rc = ensure_device(ctx);
+  if (rc) return rc;
+  rc = run_jk_device(ctx, dD, k_scale != 0.0);
+  if (rc) return rc;
+  CK(launch_fock(dH, ctx->d_Jt, k_scale != 0.0 ? ctx->d_Kt : nullptr, ctx->d_ang, ctx->nbf, k_scale, dF,
+                 ctx->stream));
+  return finish_stats(ctx);
+}
+
+int iqcp_jk(iqcp_ctx* ctx, const double* D, double* J, double* K) {
+  if (!ctx || !D || !J) return IQCP_ERR_ARG;
+  int rc = ensure_device(ctx);
+  if (rc) return rc;
+  const size_t bytes = sizeof(double) * (size_t)ctx->nbf * ctx->nbf;
+  CK(cudaMemcpyAsync(ctx->d_io[0], D, bytes, cudaMemcpyHostToDevice, ctx->stream));
+  rc = iqcp_jk_device(ctx, ctx->d_io[0], ctx->d_io[1], K ? ctx->d_io[2] : nullptr);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(J, ctx->d_io[1], bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  if (K) CK(cudaMemcpyAsync(K, ctx->d_io[2], bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return IQCP_OK;
+}
+
+int iqcp_fock(iqcp_ctx* ctx, const double* H, const double* D, double k_scale, double* F) {
+  if (!ctx || !H || !D || !F) return IQCP_ERR_ARG;
+  int rc = ensure_device(ctx);
+  if (rc) return rc;
+  const size_t bytes = sizeof(double) * (size_t)ctx->nbf * ctx->nbf;
+  CK(cudaMemcpyAsync(ctx->d_io[0], D, bytes, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->d_io[1], H, bytes, cudaMemcpyHostToDevice, ctx->stream));
+  rc = iqcp_fock_device(ctx, ctx->d_io[1], ctx->d_io[0], k_scale, ctx->d_io[2]);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(F, ctx->d_io[2], bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return IQCP_OK;
+}
+
+int iqcp_eri_grad_device(iqcp_ctx* ctx, const double* dD, double hf_frac, double* dgrad) {
+  if (!ctx || !dD || !dgrad) return IQCP_ERR_ARG;
+  int rc = ensure_device(ctx);
+  if (rc) return rc;
+  const int n = ctx->nbf;
+  CK(launch_scale_density(dD, ctx->d_ang, n, ctx->d_Ds, ctx->stream));
+  CK(cudaEventRecord(ctx->ev0, ctx->stream));
+  int launches = 0;
+  for (const TaskRange& r : ctx->ranges) {
+    if (r.count == 0) continue;
+    GradArgs a;
+    a.pairs = ctx->d_pairs;
+    a.pp = ctx->d_pp;
+    a.ket_list = ctx->d_ket_list;
+    a.tasks = ctx->d_tasks + r.first;
+    a.ntasks = r.count;
+    a.D = ctx->d_Ds;
+    a.nbf = n;
+    a.xscale = 0.25 * hf_frac;
+    a.grad = dgrad;
+    a.prim_thr = ctx->opt.prim_threshold;
+    a.schwarz_thr = ctx->opt.schwarz_threshold;
+    CK(launch_grad(r.X, r.Y, a, ctx->stream));
+    ++launches;
+  }
+  CK(cudaEventRecord(ctx->ev1, ctx->stream));
+  ctx->stats[0] = (double)ctx->n_quartets;
+  ctx->stats[1] = launches;
+  return finish_stats(ctx);
+}
+
+int iqcp_eri_grad(iqcp_ctx* ctx, const double* D, double hf_frac, double* grad) {
+  if (!ctx || !D || !grad) return IQCP_ERR_ARG;
+  int rc = ensure_device(ctx);
+  if (rc) return rc;
+  const size_t bytes = sizeof(double) * (size_t)ctx->nbf * ctx->nbf;
+  CK(cudaMemcpyAsync(ctx->d_io[0], D, bytes, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->d_grad, grad, sizeof(double) * 3 * ctx->n_atoms, cudaMemcpyHostToDevice, ctx->stream));
+  rc = iqcp_eri_grad_device(ctx, ctx->d_io[0], hf_frac, ctx->d_grad);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(grad, ctx->d_grad, sizeof(double) * 3 * ctx->n_atoms, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return IQCP_OK;
+}
+
+int iqcp_eri_compressed(iqcp_ctx* ctx, double* out, long long out_len) {
+  if (!ctx || !out) return IQCP_ERR_ARG;
+  const long long n = ctx->nbf, np = n * (n + 1) / 2, ne = np * (np + 1) / 2;
+  if (out_len < ne) return fail(ctx, IQCP_ERR_ARG, "output too small for the compressed ERI array");
+  int rc = ensure_device(ctx);
+  if (rc) return rc;
+  double* d_out = nullptr;
+  if (cudaMalloc(&d_out, sizeof(double) * ne) != cudaSuccess)
+    return fail(ctx, IQCP_ERR_NOMEM, "compressed ERI array does not fit on the device");
+  CK(cudaMemsetAsync(d_out, 0, sizeof(double) * ne, ctx->stream));
+  for (const TaskRange& r : ctx->ranges) {
+    if (r.count == 0) continue;
+    StoreArgs a;
+    a.pairs = ctx->d_pairs;
+    a.pp = ctx->d_pp;
+    a.ket_list = ctx->d_ket_list;
+    a.tasks = ctx->d_tasks + r.first;
+    a.ntasks = r.count;
+    a.out = d_out;
+    a.prim_thr = ctx->opt.prim_threshold;
+    CK(launch_store(r.X, r.Y, a, ctx->stream));
+  }
+  CK(cudaMemcpyAsync(out, d_out, sizeof(double) * ne, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  CK(cudaFree(d_out));
+  return IQCP_OK;
+}
+
+int iqcp_schwarz(iqcp_ctx* ctx, double* Q) {
+  if (!ctx || !Q) return IQCP_ERR_ARG;
+  const int ns = ctx->n_shells;
+  for (const ShellPair& p : ctx->pairs) {
+    Q[p.sa * ns + p.sb] = p.Q;
+    Q[p.sb * ns + p.sa] = p.Q;
+  }
+  return IQCP_OK;
+}
+
+int iqcp_last_stats(const iqcp_ctx* ctx, double* s) {
+  if (!ctx || !s) return IQCP_ERR_ARG;
+  for (int i = 0; i < 4; ++i) s[i] = ctx->stats[i];
+  return IQCP_OK;
+}
+
+static int batch_common(int n, const double* T) {
+  if (n <= 0 || !T) return IQCP_ERR_ARG;
+  for (int i = 0; i < n; ++i)
+    if (!(T[i] >= 0.0) || !std::isfinite(T[i])) return IQCP_ERR_ARG;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return IQCP_ERR_NODEVICE;
+  return IQCP_OK;
+}
+
+int iqcp_boys_batch(int m_max, int n, const double* T, double* F) {
+  if (m_max < 0 || m_max > 31 || !F) return IQCP_ERR_ARG;
+  int rc = batch_common(n, T);
+  if (rc) return rc;
+  double *dT = nullptr, *dF = nullptr;
+  if (cudaMalloc(&dT, sizeof(double) * n) != cudaSuccess) return IQCP_ERR_NOMEM;
+  if (cudaMalloc(&dF, sizeof(double) * n * (m_max + 1)) != cudaSuccess) { cudaFree(dT); return IQCP_ERR_NOMEM; }
+  cudaMemcpy(dT, T, sizeof(double) * n, cudaMemcpyHostToDevice);
+  cudaError_t e = launch_boys_batch(m_max, n, dT, dF, 0);
+  if (e == cudaSuccess) e = cudaMemcpy(F, dF, sizeof(double) * n * (m_max + 1), cudaMemcpyDeviceToHost);
+  cudaFree(dT);
+  cudaFree(dF);
+  return e == cudaSuccess ? IQCP_OK : IQCP_ERR_CUDA;
+}
+
+int iqcp_rys_batch(int nroots, int n, const double* T, double* roots, double* weights) {
+  if (nroots < 1 || nroots > 7 || !roots || !weights) return IQCP_ERR_ARG;
+  int rc = batch_common(n, T);
+  if (rc) return rc;
+  double *dT = nullptr, *dR = nullptr, *dW = nullptr;
+  if (cudaMalloc(&dT, sizeof(double) * n) != cudaSuccess) return IQCP_ERR_NOMEM;
+  if (cudaMalloc(&dR, sizeof(double) * n * nroots) != cudaSuccess) { cudaFree(dT); return IQCP_ERR_NOMEM; }
+  if (cudaMalloc(&dW, sizeof(double) * n * nroots) != cudaSuccess) { cudaFree(dT); cudaFree(dR); return IQCP_ERR_NOMEM; }
+  cudaMemcpy(dT, T, sizeof(double) * n, cudaMemcpyHostToDevice);
+  cudaError_t e = launch_rys_batch(nroots, n, dT, dR, dW, 0);
+  if (e == cudaSuccess) e = cudaMemcpy(roots, dR, sizeof(double) * n * nroots, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(weights, dW, sizeof(double) * n * nroots, cudaMemcpyDeviceToHost);
+  cudaFree(dT);
+  cudaFree(dR);
+  cudaFree(dW);
+  return e == cudaSuccess ? IQCP_OK : IQCP_ERR_CUDA;
+}
+
+}  // extern "C"
