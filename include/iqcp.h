@@ -135,6 +135,14 @@ int iqcp_eri_grad_device(iqcp_ctx* ctx, const double* d_D, double hf_frac, doubl
  */
 int iqcp_eri_compressed(iqcp_ctx* ctx, double* out, long long out_len);
 
+/*
+ * One-electron matrices over the context's basis, host buffers (any may be
+ * NULL): overlap S (integrals/overlap.rs:647 overlap_matrix), kinetic T and
+ * nuclear attraction V with H = T + V (integrals/hcore.rs:103 hcore_matrix,
+ * nuclear.rs:68-305).
+ */
+int iqcp_one_electron(iqcp_ctx* ctx, double* S, double* T, double* V);
+
 /* Schwarz bounds Q[n_shells*n_shells] (compute_schwarz_bounds, eri/mod.rs:1263). */
 int iqcp_schwarz(iqcp_ctx* ctx, double* Q);
 
@@ -152,6 +160,25 @@ int iqcp_rys_batch(int nroots, int n, const double* T, double* roots, double* we
  * (CUDA events on the context stream), [3] quartets evaluated in FP32.
  */
 int iqcp_last_stats(const iqcp_ctx* ctx, double* stats4);
+
+/*
+ * Measurement support (no counterpart in the reference, which has no GPU path).
+ * iqcp_set_profiling: time every quartet-kernel launch with CUDA events.
+ * iqcp_launch_profile: per launch of the last call: kind (0 J/K, 1 gradient),
+ *   bra/ket pair class, device ms, screened quartets; returns the count.
+ * iqcp_kernel_launches: kernels launched by the last call.
+ * iqcp_model_flops: algorithmic FLOPs per (bra class X, ket class Y) [6*6] of
+ *   one J/K build (kind 0) or gradient (kind 1), from the closed-form count
+ *   per surviving primitive quartet; prim_xy / quart_xy may be NULL.
+ * iqcp_measure_peak: FMA throughput probe, which = 0 FP64, 1 FP32, TFLOP/s.
+ */
+int iqcp_set_profiling(iqcp_ctx* ctx, int on);
+int iqcp_launch_profile(const iqcp_ctx* ctx, int max, int* kind, int* X, int* Y, double* ms,
+                        long long* quartets);
+int iqcp_kernel_launches(const iqcp_ctx* ctx);
+int iqcp_model_flops(iqcp_ctx* ctx, int kind, double* flops_xy, long long* prim_xy,
+                     long long* quart_xy);
+int iqcp_measure_peak(int which, double* tflops);
 
 #ifdef __cplusplus
 }

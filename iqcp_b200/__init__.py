@@ -83,10 +83,20 @@ EXPORTS = {
     "iqcp_eri_grad_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double, ctypes.c_void_p]),
     "iqcp_eri_compressed": (ctypes.c_int, [ctypes.c_void_p, _c_dbl_p, ctypes.c_longlong]),
     "iqcp_schwarz": (ctypes.c_int, [ctypes.c_void_p, _c_dbl_p]),
+    "iqcp_one_electron": (ctypes.c_int, [ctypes.c_void_p, _c_dbl_p, _c_dbl_p, _c_dbl_p]),
     "iqcp_boys_batch": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _c_dbl_p, _c_dbl_p]),
     "iqcp_rys_batch": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _c_dbl_p, _c_dbl_p, _c_dbl_p]),
     "iqcp_last_stats": (ctypes.c_int, [ctypes.c_void_p, _c_dbl_p]),
+    "iqcp_set_profiling": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "iqcp_launch_profile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _c_int_p, _c_int_p, _c_int_p, _c_dbl_p,
+                                           ctypes.POINTER(ctypes.c_longlong)]),
+    "iqcp_kernel_launches": (ctypes.c_int, [ctypes.c_void_p]),
+    "iqcp_model_flops": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _c_dbl_p, ctypes.POINTER(ctypes.c_longlong),
+                                        ctypes.POINTER(ctypes.c_longlong)]),
+    "iqcp_measure_peak": (ctypes.c_int, [ctypes.c_int, _c_dbl_p]),
 }
+
+PAIR_CLASSES = ["ss", "ps", "pp", "ds", "dp", "dd"]
 
 
 def load_library():
@@ -268,10 +278,44 @@ class FockEngine:
         self._check(self._lib.iqcp_schwarz(self._h, _dp(q)))
         return q
 
+    def one_electron(self):
+        """(S, T, V) on the device: overlap_matrix / kinetic / nuclear attraction."""
+        n = self.nbf
+        S, T, V = np.empty((n, n)), np.empty((n, n)), np.empty((n, n))
+        self._check(self._lib.iqcp_one_electron(self._h, _dp(S), _dp(T), _dp(V)))
+        return S, T, V
+
     def last_stats(self):
         s = np.zeros(4)
         self._check(self._lib.iqcp_last_stats(self._h, _dp(s)))
         return {"quartets": int(s[0]), "launches": int(s[1]), "kernel_us": float(s[2]), "fp32_quartets": int(s[3])}
+
+    def set_profiling(self, on=True):
+        self._check(self._lib.iqcp_set_profiling(self._h, int(bool(on))))
+
+    def launch_profile(self):
+        """Per quartet-kernel launch of the last call: dicts with kind, class, ms, quartets."""
+        m = 64
+        kind, X, Y = (np.zeros(m, np.int32) for _ in range(3))
+        ms = np.zeros(m)
+        q = np.zeros(m, np.int64)
+        n = self._lib.iqcp_launch_profile(self._h, m, _ip(kind), _ip(X), _ip(Y), _dp(ms),
+                                          q.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong)))
+        return [{"kind": ("jk", "grad")[kind[i]], "cls": "(%s|%s)" % (PAIR_CLASSES[X[i]], PAIR_CLASSES[Y[i]]),
+                 "X": int(X[i]), "Y": int(Y[i]), "ms": float(ms[i]), "quartets": int(q[i])} for i in range(min(n, m))]
+
+    def kernel_launches(self):
+        return self._lib.iqcp_kernel_launches(self._h)
+
+    def model_flops(self, kind="jk"):
+        """Algorithmic FLOPs [6x6] per (bra, ket) pair class, surviving primitive quartets, quartets."""
+        f = np.zeros(36)
+        p = np.zeros(36, np.int64)
+        q = np.zeros(36, np.int64)
+        LL = ctypes.POINTER(ctypes.c_longlong)
+        self._check(self._lib.iqcp_model_flops(self._h, {"jk": 0, "grad": 1}[kind], _dp(f), p.ctypes.data_as(LL),
+                                               q.ctypes.data_as(LL)))
+        return f.reshape(6, 6), p.reshape(6, 6), q.reshape(6, 6)
 
     # device-resident forms (pointers to nbf*nbf doubles in HBM, e.g. torch tensors' data_ptr())
     def jk_device(self, d_D, d_J, d_K=None):
@@ -299,6 +343,16 @@ def boys_eval_all(m_max, T):
     if rc:
         raise IqcpError(rc)
     return F
+
+
+def measure_peak(which="fp64"):
+    """FMA-throughput probe on the current device, TFLOP/s."""
+    lib = load_library()
+    t = ctypes.c_double()
+    rc = lib.iqcp_measure_peak({"fp64": 0, "fp32": 1}[which], ctypes.byref(t))
+    if rc:
+        raise IqcpError(rc)
+    return t.value
 
 
 def rys_roots(nroots, T):

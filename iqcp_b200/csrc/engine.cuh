@@ -101,7 +101,23 @@ struct GradArgs {
   double schwarz_thr;
 };
 
-// Host launchers (eri_kernels.cu)
+struct OneEArgs {
+  int n_shells, n_atoms, nbf;
+  const int* l;
+  const int* nprim;
+  const int* pstart;
+  const int* off;
+  const double* center;
+  const double* exps;
+  const double* coefs;
+  const double* atom_xyz;
+  const int* z;
+  double* S;  // may be null
+  double* T;  // may be null
+  double* V;  // may be null
+};
+
+// Host launchers (eri_aux.cu, onee.cu)
 cudaError_t launch_jk(int X, int Y, const JKArgs& a, cudaStream_t st);
 cudaError_t launch_store(int X, int Y, const StoreArgs& a, cudaStream_t st);
 cudaError_t launch_grad(int X, int Y, const GradArgs& a, cudaStream_t st);
@@ -113,5 +129,11 @@ cudaError_t launch_fock(const double* H, const double* Jt, const double* Kt, con
                         double kscale, double* F, cudaStream_t st);
 cudaError_t launch_boys_batch(int m, int n, const double* T, double* F, cudaStream_t st);
 cudaError_t launch_rys_batch(int nr, int n, const double* T, double* R, double* W, cudaStream_t st);
+cudaError_t launch_one_electron(const OneEArgs& a, cudaStream_t st);
+cudaError_t launch_count_prim_quartets(const ShellPair* pairs, const PrimPair* pp, const int* ket_list,
+                                       const QuartetTask* tasks, int ntasks, double thr,
+                                       unsigned long long* out, cudaStream_t st);
+// FMA-throughput probe: which = 0 FP64, 1 FP32; returns flops done and device ms
+cudaError_t launch_fma_peak(int which, double* flops, float* ms);
 
 }  // namespace iqcp

@@ -101,6 +101,79 @@ cudaError_t launch_rys_batch(int nr, int n, const double* T, double* R, double* 
 }
 
 
+// Surviving primitive quartets (K_ij * K_kl >= thr) of a task range.
+__global__ void count_prim_quartets_kernel(const ShellPair* __restrict__ pairs, const PrimPair* __restrict__ pp,
+                                           const int* __restrict__ ket_list, const QuartetTask* __restrict__ tasks,
+                                           int ntasks, double thr, unsigned long long* out) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  unsigned long long c = 0;
+  if (warp < ntasks) {
+    const QuartetTask t = tasks[warp];
+    if (lane < t.nket) {
+      const ShellPair bp = pairs[t.bra];
+      const ShellPair kp = pairs[ket_list[t.ket0 + lane]];
+      for (int i = 0; i < bp.np; ++i) {
+        const double kb = pp[bp.pstart + i].K;
+        for (int j = 0; j < kp.np; ++j) c += (kb * pp[kp.pstart + j].K >= thr) ? 1ull : 0ull;
+      }
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+  if (lane == 0 && c) atomicAdd(out, c);
+}
+
+cudaError_t launch_count_prim_quartets(const ShellPair* pairs, const PrimPair* pp, const int* ket_list,
+                                       const QuartetTask* tasks, int ntasks, double thr,
+                                       unsigned long long* out, cudaStream_t st) {
+  count_prim_quartets_kernel<<<(ntasks + 3) / 4, 128, 0, st>>>(pairs, pp, ket_list, tasks, ntasks, thr, out);
+  return cudaGetLastError();
+}
+
+// FMA throughput probe: 8 independent chains per thread.
+template <typename T>
+__global__ void __launch_bounds__(256) fma_peak_kernel(T* out, int iters, T a, T b) {
+  T x[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) x[k] = T(threadIdx.x + k);
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) x[k] = fma(x[k], a, b);
+  }
+  T s = 0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) s += x[k];
+  if (s == T(-1.2345)) out[0] = s;  // keep the chains alive
+}
+
+cudaError_t launch_fma_peak(int which, double* flops, float* ms) {
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int blocks = sms * 8, threads = 256, iters = 1 << 15;
+  void* out = nullptr;
+  cudaError_t e = cudaMalloc(&out, 16);
+  if (e != cudaSuccess) return e;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  for (int rep = 0; rep < 2; ++rep) {  // first pass warms clocks
+    cudaEventRecord(e0);
+    if (which == 0) fma_peak_kernel<double><<<blocks, threads>>>((double*)out, iters, 0.999999, 1e-7);
+    else fma_peak_kernel<float><<<blocks, threads>>>((float*)out, iters, 0.999999f, 1e-7f);
+    cudaEventRecord(e1);
+    cudaEventSynchronize(e1);
+  }
+  e = cudaGetLastError();
+  cudaEventElapsedTime(ms, e0, e1);
+  *flops = 2.0 * 8.0 * double(iters) * double(blocks) * double(threads);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(out);
+  return e;
+}
+
 #define IQCP_DECL_BRA(NAME, ARGS)                                                \
   extern template cudaError_t NAME<0, 0>(int, const ARGS&, cudaStream_t);        \
   extern template cudaError_t NAME<1, 0>(int, const ARGS&, cudaStream_t);        \

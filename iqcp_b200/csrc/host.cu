@@ -26,6 +26,7 @@ struct ClassList {
 struct TaskRange {
   int X, Y;
   int first, count;         // into the task array
+  long long quartets;       // screened shell quartets in the range
 };
 
 }  // namespace
@@ -49,6 +50,10 @@ struct iqcp_ctx {
   double* d_Kt = nullptr;
   double* d_io[4] = {nullptr, nullptr, nullptr, nullptr};  // staging for host-buffer calls
   double* d_grad = nullptr;
+  // basis copy for the one-electron kernel
+  int* d_bint = nullptr;          // l | nprim | pstart | off | z
+  double* d_bdbl = nullptr;       // center | exps | coefs | atom_xyz
+  int n_prims = 0;
   // host copies
   std::vector<ShellPair> pairs;
   std::vector<int> list_offset;   // per class, into d_ket_list
@@ -57,6 +62,14 @@ struct iqcp_ctx {
   long long n_quartets = 0;
   double stats[4] = {0, 0, 0, 0};
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // per-launch timing of the quartet kernels (off unless requested)
+  bool profile = false;
+  std::vector<cudaEvent_t> pev;
+  struct LaunchRec { int kind, X, Y; float ms; long long quartets; };
+  std::vector<LaunchRec> launch_log;
+  int launches_total = 0;       // every kernel of the last call
+  // surviving primitive quartets per task range (counted on first request)
+  std::vector<long long> prim_quartets;
 };
 
 namespace {
@@ -127,7 +140,7 @@ void build_tasks(iqcp_ctx* ctx, std::vector<int>& ket_list, std::vector<QuartetT
     for (int Y = 0; Y <= X; ++Y) {
       const auto& LX = ctx->classes[X].pairs;
       const auto& LY = ctx->classes[Y].pairs;
-      TaskRange r{X, Y, (int)tasks.size(), 0};
+      TaskRange r{X, Y, (int)tasks.size(), 0, 0};
       for (int b = 0; b < (int)LX.size(); ++b) {
         const double qb = ctx->pairs[LX[b]].Q;
         // ket prefix with qb*qk >= thr (lists sorted by Q descending)
@@ -139,6 +152,7 @@ void build_tasks(iqcp_ctx* ctx, std::vector<int>& ket_list, std::vector<QuartetT
         int nk = lo;
         if (X == Y) nk = std::min(nk, b + 1);
         ctx->n_quartets += nk;
+        r.quartets += nk;
         for (int k0 = 0; k0 < nk; k0 += 32) {
           QuartetTask t;
           t.bra = LX[b];
@@ -160,16 +174,50 @@ int ensure_device(iqcp_ctx* ctx) {
   return IQCP_OK;
 }
 
+int ensure_profile_events(iqcp_ctx* ctx) {
+  const size_t need = 2 * ctx->ranges.size();
+  while (ctx->pev.size() < need) {
+    cudaEvent_t e;
+    CK(cudaEventCreate(&e));
+    ctx->pev.push_back(e);
+  }
+  return IQCP_OK;
+}
+
+// Launch one quartet kernel per non-empty class range; kind 0 = J/K, 1 = gradient.
+template <typename F>
+int run_ranges(iqcp_ctx* ctx, int kind, F&& launch) {
+  if (ctx->profile) {
+    int rc = ensure_profile_events(ctx);
+    if (rc) return rc;
+  }
+  ctx->launch_log.clear();
+  CK(cudaEventRecord(ctx->ev0, ctx->stream));
+  int launches = 0;
+  for (size_t i = 0; i < ctx->ranges.size(); ++i) {
+    const TaskRange& r = ctx->ranges[i];
+    if (r.count == 0) continue;
+    if (ctx->profile) CK(cudaEventRecord(ctx->pev[2 * i], ctx->stream));
+    CK(launch(r));
+    if (ctx->profile) CK(cudaEventRecord(ctx->pev[2 * i + 1], ctx->stream));
+    ++launches;
+    ctx->launch_log.push_back({kind, r.X, r.Y, 0.f, r.quartets});
+  }
+  CK(cudaEventRecord(ctx->ev1, ctx->stream));
+  ctx->stats[0] = (double)ctx->n_quartets;
+  ctx->stats[1] = launches;
+  ctx->launches_total += launches;
+  return IQCP_OK;
+}
+
 int run_jk_device(iqcp_ctx* ctx, const double* dD, bool want_k) {
   const int n = ctx->nbf;
   const size_t bytes = sizeof(double) * (size_t)n * n;
+  ctx->launches_total = 1;
   CK(launch_scale_density(dD, ctx->d_ang, n, ctx->d_Ds, ctx->stream));
   CK(cudaMemsetAsync(ctx->d_Jt, 0, bytes, ctx->stream));
   if (want_k) CK(cudaMemsetAsync(ctx->d_Kt, 0, bytes, ctx->stream));
-  CK(cudaEventRecord(ctx->ev0, ctx->stream));
-  int launches = 0;
-  for (const TaskRange& r : ctx->ranges) {
-    if (r.count == 0) continue;
+  return run_ranges(ctx, 0, [&](const TaskRange& r) {
     JKArgs a;
     a.pairs = ctx->d_pairs;
     a.pp = ctx->d_pp;
@@ -181,13 +229,8 @@ int run_jk_device(iqcp_ctx* ctx, const double* dD, bool want_k) {
     a.J = ctx->d_Jt;
     a.K = want_k ? ctx->d_Kt : nullptr;
     a.prim_thr = ctx->opt.prim_threshold;
-    CK(launch_jk(r.X, r.Y, a, ctx->stream));
-    ++launches;
-  }
-  CK(cudaEventRecord(ctx->ev1, ctx->stream));
-  ctx->stats[0] = (double)ctx->n_quartets;
-  ctx->stats[1] = launches;
-  return IQCP_OK;
+    return launch_jk(r.X, r.Y, a, ctx->stream);
+  });
 }
 
 int finish_stats(iqcp_ctx* ctx) {
@@ -195,6 +238,15 @@ int finish_stats(iqcp_ctx* ctx) {
   CK(cudaEventSynchronize(ctx->ev1));
   CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
   ctx->stats[2] = ms * 1e3;
+  if (ctx->profile) {
+    size_t k = 0;
+    for (size_t i = 0; i < ctx->ranges.size(); ++i) {
+      if (ctx->ranges[i].count == 0) continue;
+      float t = 0.f;
+      CK(cudaEventElapsedTime(&t, ctx->pev[2 * i], ctx->pev[2 * i + 1]));
+      ctx->launch_log[k++].ms = t;
+    }
+  }
   return IQCP_OK;
 }
 
@@ -280,7 +332,31 @@ int iqcp_create(const iqcp_basis_desc* b, const iqcp_options* opts, iqcp_ctx** o
     pstart[s + 1] = pstart[s] + b->nprim[s];
   }
   ctx->nbf = off;
+  ctx->n_prims = pstart[b->n_shells];
   const double kthr = ctx->opt.prim_threshold;
+  for (int s = 0; s < b->n_shells; ++s)
+    for (int d = 0; d < 3; ++d)
+      if (!std::isfinite(b->center[3 * s + d])) return fail(ctx, IQCP_ERR_NUMERIC, "non-finite shell centre");
+  for (int p = 0; p < ctx->n_prims; ++p)
+    if (!(b->exps[p] > 0.0) || !std::isfinite(b->coefs[p])) return fail(ctx, IQCP_ERR_ARG, "bad primitive");
+  {
+    const int ns = b->n_shells, na = b->n_atoms;
+    std::vector<int> bi;
+    bi.insert(bi.end(), b->l, b->l + ns);
+    bi.insert(bi.end(), b->nprim, b->nprim + ns);
+    bi.insert(bi.end(), pstart.begin(), pstart.begin() + ns);
+    bi.insert(bi.end(), ctx->shell_off.begin(), ctx->shell_off.end());
+    bi.insert(bi.end(), b->z, b->z + na);
+    std::vector<double> bd;
+    bd.insert(bd.end(), b->center, b->center + 3 * ns);
+    bd.insert(bd.end(), b->exps, b->exps + ctx->n_prims);
+    bd.insert(bd.end(), b->coefs, b->coefs + ctx->n_prims);
+    bd.insert(bd.end(), b->atom_xyz, b->atom_xyz + 3 * na);
+    CK(cudaMalloc(&ctx->d_bint, sizeof(int) * bi.size()));
+    CK(cudaMalloc(&ctx->d_bdbl, sizeof(double) * bd.size()));
+    CK(cudaMemcpy(ctx->d_bint, bi.data(), sizeof(int) * bi.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->d_bdbl, bd.data(), sizeof(double) * bd.size(), cudaMemcpyHostToDevice));
+  }
 
   // shell pairs si >= sj (reference order), A = higher-L shell
   std::vector<PrimPair> pps;
@@ -387,6 +463,8 @@ void iqcp_destroy(iqcp_ctx* ctx) {
   cudaFree(ctx->d_Kt);
   for (int i = 0; i < 4; ++i) cudaFree(ctx->d_io[i]);
   cudaFree(ctx->d_grad);
+  cudaFree(ctx->d_bint);
+  cudaFree(ctx->d_bdbl);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
@@ -406,7 +484,11 @@ int iqcp_jk_device(iqcp_ctx* ctx, const double* dD, double* dJ, double* dK) {
   rc = run_jk_device(ctx, dD, dK != nullptr);
   if (rc) return rc;
   CK(launch_symmetrize(ctx->d_Jt, ctx->d_ang, ctx->nbf, dJ, ctx->stream));
-  if (dK) CK(launch_symmetrize(ctx->d_Kt, ctx->d_ang, ctx->nbf, dK, ctx->stream));
+  ctx->launches_total += 1;
+  if (dK) {
+    CK(launch_symmetrize(ctx->d_Kt, ctx->d_ang, ctx->nbf, dK, ctx->stream));
+    ctx->launches_total += 1;
+  }
   return finish_stats(ctx);
 }
 
@@ -418,6 +500,7 @@ int iqcp_fock_device(iqcp_ctx* ctx, const double* dH, const double* dD, double k
   if (rc) return rc;
   CK(launch_fock(dH, ctx->d_Jt, k_scale != 0.0 ? ctx->d_Kt : nullptr, ctx->d_ang, ctx->nbf, k_scale, dF,
                  ctx->stream));
+  ctx->launches_total += 1;
   return finish_stats(ctx);
 }
 
@@ -454,11 +537,9 @@ int iqcp_eri_grad_device(iqcp_ctx* ctx, const double* dD, double hf_frac, double
   int rc = ensure_device(ctx);
   if (rc) return rc;
   const int n = ctx->nbf;
+  ctx->launches_total = 1;
   CK(launch_scale_density(dD, ctx->d_ang, n, ctx->d_Ds, ctx->stream));
-  CK(cudaEventRecord(ctx->ev0, ctx->stream));
-  int launches = 0;
-  for (const TaskRange& r : ctx->ranges) {
-    if (r.count == 0) continue;
+  rc = run_ranges(ctx, 1, [&](const TaskRange& r) {
     GradArgs a;
     a.pairs = ctx->d_pairs;
     a.pp = ctx->d_pp;
@@ -471,12 +552,9 @@ int iqcp_eri_grad_device(iqcp_ctx* ctx, const double* dD, double hf_frac, double
     a.grad = dgrad;
     a.prim_thr = ctx->opt.prim_threshold;
     a.schwarz_thr = ctx->opt.schwarz_threshold;
-    CK(launch_grad(r.X, r.Y, a, ctx->stream));
-    ++launches;
-  }
-  CK(cudaEventRecord(ctx->ev1, ctx->stream));
-  ctx->stats[0] = (double)ctx->n_quartets;
-  ctx->stats[1] = launches;
+    return launch_grad(r.X, r.Y, a, ctx->stream);
+  });
+  if (rc) return rc;
   return finish_stats(ctx);
 }
 
@@ -522,6 +600,36 @@ int iqcp_eri_compressed(iqcp_ctx* ctx, double* out, long long out_len) {
   return IQCP_OK;
 }
 
+int iqcp_one_electron(iqcp_ctx* ctx, double* S, double* T, double* V) {
+  if (!ctx) return IQCP_ERR_ARG;
+  int rc = ensure_device(ctx);
+  if (rc) return rc;
+  const int ns = ctx->n_shells, na = ctx->n_atoms;
+  const size_t bytes = sizeof(double) * (size_t)ctx->nbf * ctx->nbf;
+  OneEArgs a;
+  a.n_shells = ns;
+  a.n_atoms = na;
+  a.nbf = ctx->nbf;
+  a.l = ctx->d_bint;
+  a.nprim = ctx->d_bint + ns;
+  a.pstart = ctx->d_bint + 2 * ns;
+  a.off = ctx->d_bint + 3 * ns;
+  a.z = ctx->d_bint + 4 * ns;
+  a.center = ctx->d_bdbl;
+  a.exps = ctx->d_bdbl + 3 * ns;
+  a.coefs = a.exps + ctx->n_prims;
+  a.atom_xyz = a.coefs + ctx->n_prims;
+  a.S = S ? ctx->d_io[0] : nullptr;
+  a.T = T ? ctx->d_io[1] : nullptr;
+  a.V = V ? ctx->d_io[2] : nullptr;
+  CK(launch_one_electron(a, ctx->stream));
+  if (S) CK(cudaMemcpyAsync(S, ctx->d_io[0], bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  if (T) CK(cudaMemcpyAsync(T, ctx->d_io[1], bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  if (V) CK(cudaMemcpyAsync(V, ctx->d_io[2], bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return IQCP_OK;
+}
+
 int iqcp_schwarz(iqcp_ctx* ctx, double* Q) {
   if (!ctx || !Q) return IQCP_ERR_ARG;
   const int ns = ctx->n_shells;
@@ -529,6 +637,122 @@ int iqcp_schwarz(iqcp_ctx* ctx, double* Q) {
     Q[p.sa * ns + p.sb] = p.Q;
     Q[p.sb * ns + p.sa] = p.Q;
   }
+  return IQCP_OK;
+}
+
+int iqcp_set_profiling(iqcp_ctx* ctx, int on) {
+  if (!ctx) return IQCP_ERR_ARG;
+  ctx->profile = on != 0;
+  return IQCP_OK;
+}
+
+int iqcp_launch_profile(const iqcp_ctx* ctx, int max, int* kind, int* X, int* Y, double* ms,
+                        long long* quartets) {
+  if (!ctx) return IQCP_ERR_ARG;
+  const int n = (int)ctx->launch_log.size();
+  for (int i = 0; i < n && i < max; ++i) {
+    kind[i] = ctx->launch_log[i].kind;
+    X[i] = ctx->launch_log[i].X;
+    Y[i] = ctx->launch_log[i].Y;
+    ms[i] = ctx->launch_log[i].ms;
+    quartets[i] = ctx->launch_log[i].quartets;
+  }
+  return n;
+}
+
+int iqcp_kernel_launches(const iqcp_ctx* ctx) { return ctx ? ctx->launches_total : 0; }
+
+static int count_prim_quartets(iqcp_ctx* ctx) {
+  if (!ctx->prim_quartets.empty()) return IQCP_OK;
+  unsigned long long* d_cnt = nullptr;
+  const size_t nr = ctx->ranges.size();
+  CK(cudaMalloc(&d_cnt, sizeof(unsigned long long) * (nr + 1)));
+  CK(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long) * (nr + 1), ctx->stream));
+  for (size_t i = 0; i < nr; ++i) {
+    const TaskRange& r = ctx->ranges[i];
+    if (r.count == 0) continue;
+    CK(launch_count_prim_quartets(ctx->d_pairs, ctx->d_pp, ctx->d_ket_list, ctx->d_tasks + r.first, r.count,
+                                  ctx->opt.prim_threshold, d_cnt + i, ctx->stream));
+  }
+  std::vector<unsigned long long> h(nr + 1);
+  CK(cudaMemcpyAsync(h.data(), d_cnt, sizeof(unsigned long long) * (nr + 1), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  CK(cudaFree(d_cnt));
+  ctx->prim_quartets.assign(h.begin(), h.begin() + nr);
+  return IQCP_OK;
+}
+
+// Closed-form algorithmic FLOP model per surviving primitive quartet of class
+// (la lb|lc ld), counting the recurrences as the reference writes them
+// (vrr_2d.rs:169-193, iterative transfer htr_4d.rs:107-224) -- FMA = 2:
+//   F = 40 + sum_roots [17 + 3 VRR(nb,nk) + sum_comp (sum_axes HTR1(j,l) + 8)]
+//   VRR(nb,nk) = 4 max(nb-1,0) + [nk>0](1 + 4(nk-1)) + 7 nb nk
+//   HTR1(j,l)  = (j+1) l (l+1) + j (j+1)
+// plus 12 per contracted integral for the 8-fold J/K digestion.  Gradient:
+// tables extended by one on bra and ket, one more root, and per component
+// 4 centres x 3 axes of (2 HTR1 + 7), digested with 12 FMAs per component.
+static double vrr_cost(int nb, int nk) {
+  return 4.0 * (nb > 1 ? nb - 1 : 0) + (nk > 0 ? 1.0 + 4.0 * (nk - 1) : 0.0) + 7.0 * nb * nk;
+}
+static double htr1(int j, int l) { return double((j + 1) * l * (l + 1) + j * (j + 1)); }
+
+static void class_cost(int X, int Y, bool grad, double* per_prim, double* per_quartet) {
+  const int la = class_la(X), lb = class_lb(X), lc = class_la(Y), ld = class_lb(Y);
+  const int L = la + lb + lc + ld;
+  const int nr = grad ? (L + 2) / 2 + 1 : L / 2 + 1;
+  const int nb = la + lb + (grad ? 1 : 0), nk = lc + ld + (grad ? 1 : 0);
+  double comp = 0.0;
+  int ncomp = 0;
+  for (int a = 0; a < ncart(la); ++a)
+    for (int b = 0; b < ncart(lb); ++b)
+      for (int c = 0; c < ncart(lc); ++c)
+        for (int d = 0; d < ncart(ld); ++d) {
+          ++ncomp;
+          double s = 8.0;
+          for (int ax = 0; ax < 3; ++ax) {
+            const int j = cart_pow(lb, b, ax), l = cart_pow(ld, d, ax);
+            s += htr1(j, l);
+            // centres A, C shift i or k (cost of HTR1(j,l)); B shifts j; D shifts l
+            if (grad) s += (2.0 * htr1(j, l) + 7.0) + (2.0 * htr1(j + 1, l) + 7.0) +
+                           (2.0 * htr1(j, l) + 7.0) + (2.0 * htr1(j, l + 1) + 7.0);
+          }
+          comp += s;
+        }
+  *per_prim = 40.0 + nr * (17.0 + 3.0 * vrr_cost(nb, nk) + comp);
+  *per_quartet = (grad ? 24.0 : 12.0) * ncomp;
+}
+
+int iqcp_model_flops(iqcp_ctx* ctx, int kind, double* flops_xy, long long* prim_xy, long long* quart_xy) {
+  if (!ctx || !flops_xy) return IQCP_ERR_ARG;
+  int rc = ensure_device(ctx);
+  if (rc) return rc;
+  rc = count_prim_quartets(ctx);
+  if (rc) return rc;
+  for (int i = 0; i < kNumPairClasses * kNumPairClasses; ++i) {
+    flops_xy[i] = 0.0;
+    if (prim_xy) prim_xy[i] = 0;
+    if (quart_xy) quart_xy[i] = 0;
+  }
+  for (size_t i = 0; i < ctx->ranges.size(); ++i) {
+    const TaskRange& r = ctx->ranges[i];
+    double pp, pq;
+    class_cost(r.X, r.Y, kind == 1, &pp, &pq);
+    const int o = r.X * kNumPairClasses + r.Y;
+    flops_xy[o] = pp * (double)ctx->prim_quartets[i] + pq * (double)r.quartets;
+    if (prim_xy) prim_xy[o] = ctx->prim_quartets[i];
+    if (quart_xy) quart_xy[o] = r.quartets;
+  }
+  return IQCP_OK;
+}
+
+int iqcp_measure_peak(int which, double* tflops) {
+  if (!tflops) return IQCP_ERR_ARG;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return IQCP_ERR_NODEVICE;
+  double flops = 0.0;
+  float ms = 0.f;
+  if (launch_fma_peak(which, &flops, &ms) != cudaSuccess) return IQCP_ERR_CUDA;
+  *tflops = flops / (ms * 1e-3) * 1e-12;
   return IQCP_OK;
 }
 
