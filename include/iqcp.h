@@ -117,6 +117,21 @@ int iqcp_fock_device(iqcp_ctx* ctx, const double* d_H, const double* d_D, double
                      double* d_F);
 
 /*
+ * iqcp_jk_device without any device allocation: same inputs, outputs and
+ * results, but its scratch (scaled density, J/K accumulators) lives in a
+ * fixed file-scope device array instead of context buffers.  No counterpart
+ * in the reference.  For callers whose Fock-build loop may not call cudaMalloc
+ * (all of HBM handed to their own pool, or no implicit device synchronisation
+ * allowed); the context is created beforehand by iqcp_create.
+ * Limit: nbf <= 512 (3*512*512 doubles, 6 MiB held on every GPU that loads the
+ * library); larger bases return IQCP_ERR_ARG.  The first call on a device
+ * looks up the array's address (cudaGetSymbolAddress) -- make it before any
+ * stream capture.  All calls share the array: calls that overlap on the GPU
+ * race, so serialise them.
+ */
+int iqcp_jk_device_noalloc(iqcp_ctx* ctx, const double* d_D, double* d_J, double* d_K);
+
+/*
  * Two-electron part of the nuclear gradient, host buffers:
  * grad[3*atom + dir] += sum over unique quartets of w * d(ij|kl)/dR with
  * w = sum_perm [1/2 D_ij D_kl - 1/4 hf_frac D_ik D_jl].

@@ -87,6 +87,7 @@ EXPORTS = {
     "iqcp_boys_batch": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _c_dbl_p, _c_dbl_p]),
     "iqcp_rys_batch": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _c_dbl_p, _c_dbl_p, _c_dbl_p]),
     "iqcp_last_stats": (ctypes.c_int, [ctypes.c_void_p, _c_dbl_p]),
+    "iqcp_jk_device_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "iqcp_set_profiling": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "iqcp_launch_profile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _c_int_p, _c_int_p, _c_int_p, _c_dbl_p,
                                            ctypes.POINTER(ctypes.c_longlong)]),
@@ -321,6 +322,11 @@ class FockEngine:
     def jk_device(self, d_D, d_J, d_K=None):
         self._check(self._lib.iqcp_jk_device(self._h, ctypes.c_void_p(d_D), ctypes.c_void_p(d_J),
                                              ctypes.c_void_p(d_K) if d_K else None))
+
+    def jk_device_noalloc(self, d_D, d_J, d_K=None):
+        """iqcp_jk_device with its scratch in a fixed device array (nbf <= 512): allocates nothing."""
+        self._check(self._lib.iqcp_jk_device_noalloc(self._h, ctypes.c_void_p(d_D), ctypes.c_void_p(d_J),
+                                                     ctypes.c_void_p(d_K) if d_K else None))
 
     def fock_device(self, d_H, d_D, k_scale, d_F):
         self._check(self._lib.iqcp_fock_device(self._h, ctypes.c_void_p(d_H), ctypes.c_void_p(d_D),

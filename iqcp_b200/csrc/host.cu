@@ -504,6 +504,99 @@ int iqcp_fock_device(iqcp_ctx* ctx, const double* dH, const double* dD, double k
   return finish_stats(ctx);
 }
 
+// ---------------------------------------------------------------------------
+// J/K build that allocates nothing.
+//
+// Some callers cannot call cudaMalloc at the point where they need a Fock
+// build: a serving process that has handed all of HBM to its own memory pool
+// (a cudaMalloc there fails), or a solver loop that must not stall on the
+// implicit device synchronisation an allocation can cause.  For them this
+// entry point keeps its scratch -- the angular-scaled density and the two
+// unsymmetrised J/K accumulators -- in one file-scope device array of fixed
+// size instead of the context's own buffers.  The context itself (pair tables,
+// quartet lists) is built beforehand by iqcp_create, where allocation is
+// allowed.
+//
+// Limits and rules:
+//   * nbf <= IQCP_NOALLOC_MAX_NBF (512): the array holds 3 * 512 * 512 doubles
+//     (6 MiB), reserved on every GPU that loads the library until exit;
+//     larger bases are rejected with IQCP_ERR_ARG.
+//   * The first call on a device looks up the array's device address with
+//     cudaGetSymbolAddress (once per device, with that device current); make
+//     that first call before any stream capture.
+//   * All calls share the one array, which keeps the last call's contents;
+//     the accumulators are cleared at the start of every call.  Calls whose
+//     work overlaps on the GPU (other streams, other host threads) race on the
+//     array: serialise them.
+#define IQCP_NOALLOC_MAX_NBF 512
+static __device__ __align__(256) double g_noalloc_scratch[3 * IQCP_NOALLOC_MAX_NBF * IQCP_NOALLOC_MAX_NBF];
+static double* g_noalloc_ptr[64] = {nullptr};
+
+static int noalloc_scratch(iqcp_ctx* ctx, double** out) {
+  if (ctx->device < 0 || ctx->device >= 64) return fail(ctx, IQCP_ERR_ARG, "device ordinal out of range");
+  if (!g_noalloc_ptr[ctx->device]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+      return fail(ctx, IQCP_ERR_CUDA, std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") +
+                                          cudaGetErrorString(e));
+    g_noalloc_ptr[ctx->device] = static_cast<double*>(p);
+  }
+  *out = g_noalloc_ptr[ctx->device];
+  return IQCP_OK;
+}
+
+int iqcp_jk_device_noalloc(iqcp_ctx* ctx, const double* dD, double* dJ, double* dK) {
+  if (!ctx || !dD || !dJ) return IQCP_ERR_ARG;
+  if (ctx->nbf > IQCP_NOALLOC_MAX_NBF)
+    return fail(ctx, IQCP_ERR_ARG, "iqcp_jk_device_noalloc supports nbf <= 512 (static scratch size); nbf = " +
+                                       std::to_string(ctx->nbf));
+  int rc = ensure_device(ctx);
+  if (rc) return rc;
+  double* scratch = nullptr;
+  rc = noalloc_scratch(ctx, &scratch);
+  if (rc) return rc;
+  const int n = ctx->nbf;
+  const size_t nn = (size_t)n * n;
+  double* Ds = scratch;
+  double* Jt = scratch + nn;
+  double* Kt = scratch + 2 * nn;
+  const bool want_k = dK != nullptr;
+  const bool prof = ctx->profile;
+  ctx->profile = false;  // per-launch timing would create events
+  ctx->launches_total = 1;
+  CK(launch_scale_density(dD, ctx->d_ang, n, Ds, ctx->stream));
+  CK(cudaMemsetAsync(Jt, 0, sizeof(double) * nn, ctx->stream));
+  if (want_k) CK(cudaMemsetAsync(Kt, 0, sizeof(double) * nn, ctx->stream));
+  rc = run_ranges(ctx, 0, [&](const TaskRange& r) {
+    JKArgs a;
+    a.pairs = ctx->d_pairs;
+    a.pp = ctx->d_pp;
+    a.ket_list = ctx->d_ket_list;
+    a.tasks = ctx->d_tasks + r.first;
+    a.ntasks = r.count;
+    a.D = Ds;
+    a.nbf = n;
+    a.J = Jt;
+    a.K = want_k ? Kt : nullptr;
+    a.prim_thr = ctx->opt.prim_threshold;
+    return launch_jk(r.X, r.Y, a, ctx->stream);
+  });
+  ctx->profile = prof;
+  if (rc) return rc;
+  CK(launch_symmetrize(Jt, ctx->d_ang, n, dJ, ctx->stream));
+  ctx->launches_total += 1;
+  if (want_k) {
+    CK(launch_symmetrize(Kt, ctx->d_ang, n, dK, ctx->stream));
+    ctx->launches_total += 1;
+  }
+  float ms = 0.f;
+  CK(cudaEventSynchronize(ctx->ev1));
+  CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+  ctx->stats[2] = ms * 1e3;
+  return IQCP_OK;
+}
+
 int iqcp_jk(iqcp_ctx* ctx, const double* D, double* J, double* K) {
   if (!ctx || !D || !J) return IQCP_ERR_ARG;
   int rc = ensure_device(ctx);
