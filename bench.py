@@ -213,6 +213,8 @@ def main():
         p2 = eng.launch_profile()
         return l1 + l2 + 1, p1 + p2
 
+    # kernel variant per class, picked on this density (set-up, not timed)
+    modes = eng.autotune(dD.data_ptr(), 2)
     for _ in range(args.warmup):
         step()
     eng.set_profiling(True)
@@ -300,6 +302,9 @@ def main():
         "clocks": clocks, "gpu_launches": launches,
         "kernels": {"%s %s" % (k[0], v[2]): round(v[0] / v[1], 4) for k, v in sorted(per_kernel.items())},
         "scf": {"energy": scf.energy, "iterations": scf.iterations, "converged": bool(scf.converged)},
+        "kernel_modes": {"jk": modes[0].tolist(), "grad": modes[1].tolist(),
+                         "legend": "rows bra class, cols ket class (ss ps pp ds dp dd); 0 thread/quartet, "
+                                   "1 warp/quartet, 2 8 lanes/quartet, 3 32 lanes/quartet"},
     }
     jk_ms = sum(v[0] / v[1] for k, v in per_kernel.items() if k[0] == "jk")
     gr_ms = sum(v[0] / v[1] for k, v in per_kernel.items() if k[0] == "grad")

@@ -93,6 +93,13 @@ void iqcp_destroy(iqcp_ctx* ctx);
 const char* iqcp_last_error(const iqcp_ctx* ctx);
 int iqcp_nbf(const iqcp_ctx* ctx);
 
+/*
+ * Switch the context between the FP64 form and the mixed form (quartets with
+ * Q_ij*Q_kl*max|D| below mixed_cutoff run their quadrature in FP32; Rys roots
+ * and weights, recurrence coefficients and all accumulation stay FP64).
+ */
+int iqcp_set_precision(iqcp_ctx* ctx, int precision, double mixed_cutoff);
+
 /* Run the context's work on this CUDA stream (cudaStream_t); NULL = its own stream. */
 int iqcp_set_stream(iqcp_ctx* ctx, void* stream);
 
@@ -194,6 +201,19 @@ int iqcp_kernel_launches(const iqcp_ctx* ctx);
 int iqcp_model_flops(iqcp_ctx* ctx, int kind, double* flops_xy, long long* prim_xy,
                      long long* quart_xy);
 int iqcp_measure_peak(int which, double* tflops);
+
+/*
+ * Kernel-variant autotuner (no reference counterpart): for every (bra class,
+ * ket class) time each quartet-kernel variant (0: one quartet per thread,
+ * 1: one warp per quartet with shared-memory 1D tables) on this device-resident
+ * density, best of `reps`, and keep the fastest for J/K and for gradients.
+ * Results agree to rounding whichever variant runs.  iqcp_kernel_modes returns
+ * the choice as modes[(kind*6 + X)*6 + Y] (-1: class has no quartets);
+ * iqcp_set_kernel_mode forces one (X or Y = -1: all classes).
+ */
+int iqcp_autotune(iqcp_ctx* ctx, const double* d_D, int reps);
+int iqcp_kernel_modes(const iqcp_ctx* ctx, int* modes);
+int iqcp_set_kernel_mode(iqcp_ctx* ctx, int kind, int X, int Y, int mode);
 
 #ifdef __cplusplus
 }

@@ -74,6 +74,7 @@ EXPORTS = {
     "iqcp_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
     "iqcp_nbf": (ctypes.c_int, [ctypes.c_void_p]),
     "iqcp_set_stream": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "iqcp_set_precision": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_double]),
     "iqcp_jk": (ctypes.c_int, [ctypes.c_void_p, _c_dbl_p, _c_dbl_p, _c_dbl_p]),
     "iqcp_fock": (ctypes.c_int, [ctypes.c_void_p, _c_dbl_p, _c_dbl_p, ctypes.c_double, _c_dbl_p]),
     "iqcp_jk_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
@@ -95,6 +96,9 @@ EXPORTS = {
     "iqcp_model_flops": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _c_dbl_p, ctypes.POINTER(ctypes.c_longlong),
                                         ctypes.POINTER(ctypes.c_longlong)]),
     "iqcp_measure_peak": (ctypes.c_int, [ctypes.c_int, _c_dbl_p]),
+    "iqcp_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]),
+    "iqcp_kernel_modes": (ctypes.c_int, [ctypes.c_void_p, _c_int_p]),
+    "iqcp_set_kernel_mode": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
 }
 
 PAIR_CLASSES = ["ss", "ps", "pp", "ds", "dp", "dd"]
@@ -305,6 +309,19 @@ class FockEngine:
         return [{"kind": ("jk", "grad")[kind[i]], "cls": "(%s|%s)" % (PAIR_CLASSES[X[i]], PAIR_CLASSES[Y[i]]),
                  "X": int(X[i]), "Y": int(Y[i]), "ms": float(ms[i]), "quartets": int(q[i])} for i in range(min(n, m))]
 
+    def autotune(self, d_D, reps=2):
+        """Pick the fastest quartet-kernel variant per class on this device density pointer."""
+        self._check(self._lib.iqcp_autotune(self._h, ctypes.c_void_p(d_D), int(reps)))
+        return self.kernel_modes()
+
+    def kernel_modes(self):
+        m = np.zeros(72, np.int32)
+        self._check(self._lib.iqcp_kernel_modes(self._h, _ip(m)))
+        return m.reshape(2, 6, 6)
+
+    def set_kernel_mode(self, kind, X=-1, Y=-1, mode=0):
+        self._check(self._lib.iqcp_set_kernel_mode(self._h, {"jk": 0, "grad": 1}[kind], X, Y, mode))
+
     def kernel_launches(self):
         return self._lib.iqcp_kernel_launches(self._h)
 
@@ -335,6 +352,10 @@ class FockEngine:
     def eri_gradient_device(self, d_D, hf_frac, d_grad):
         self._check(self._lib.iqcp_eri_grad_device(self._h, ctypes.c_void_p(d_D), float(hf_frac),
                                                    ctypes.c_void_p(d_grad)))
+
+    def set_precision(self, precision, mixed_cutoff=1e-9):
+        """FP64 (0) or MIXED (1): FP32 quadrature for quartets with Q_ij Q_kl max|D| < mixed_cutoff."""
+        self._check(self._lib.iqcp_set_precision(self._h, int(precision), float(mixed_cutoff)))
 
     def set_stream(self, stream_handle):
         self._check(self._lib.iqcp_set_stream(self._h, ctypes.c_void_p(stream_handle)))

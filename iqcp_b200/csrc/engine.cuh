@@ -7,6 +7,14 @@
 
 namespace iqcp {
 
+constexpr int kNumModes = 4;  // quartet-kernel variants per class
+
+// Default variant before autotuning: warp-cooperative for component-rich
+// classes, one quartet per thread for the rest.
+__host__ __device__ constexpr int default_mode(int X, int Y, int kind) {
+  return ((X == 5 || (X == 4 && Y >= 2)) && !(kind == 1 && X == 4 && Y == 3)) ? 1 : 0;
+}
+
 // Angular-momentum classes of a shell pair with la >= lb:
 // 0 ss, 1 ps, 2 pp, 3 ds, 4 dp, 5 dd  (index la*(la+1)/2 + lb)
 constexpr int kNumPairClasses = 6;
@@ -34,8 +42,8 @@ struct __align__(16) PrimPair {
   double P[3];    // Gaussian product centre
   double K;       // exp(-alpha_a alpha_b / p |AB|^2)  (screening value)
   double cK;      // K * c_a * c_b * Nrad(alpha_a, la) * Nrad(alpha_b, lb)
-  double aa;      // alpha_a
-  double ab;      // alpha_b
+  double aa;      // alpha_a (alpha_b = p - alpha_a)
+  double inv_p;   // 1 / p
 };
 
 // One shell pair (la >= lb after the swap), 64 bytes.
@@ -63,6 +71,14 @@ struct QuartetTask {
   int flags;      // bit0: evaluate in FP32 (mixed precision)
 };
 
+// Dynamic task distribution of the persistent quartet kernels: lane 0 of a
+// warp takes the next task index from the launch's counter.
+__device__ __forceinline__ int next_task(int* counter, int lane) {
+  int t = 0;
+  if (lane == 0) t = atomicAdd(counter, 1);
+  return __shfl_sync(0xffffffffu, t, 0);
+}
+
 // Kernel argument blocks (passed by value).
 struct JKArgs {
   const ShellPair* pairs;
@@ -75,6 +91,13 @@ struct JKArgs {
   double* J;         // unsymmetrised accumulators (nbf x nbf)
   double* K;         // may be null
   double prim_thr;
+  int mode;          // kernel variant: 0 thread per quartet, 1 warp-cooperative, 2/3: 8/32 lanes per quartet
+  // mixed precision (null dmax_shell: all FP64)
+  const double* dmax_shell;   // max |D| per shell-pair block, n_shells x n_shells
+  int n_shells;
+  double mixed_cutoff;
+  unsigned long long* fp32_count;
+  int* next_task;             // work counter (zeroed before the launch)
 };
 
 struct StoreArgs {
@@ -99,6 +122,10 @@ struct GradArgs {
   double* grad;      // natoms x 3
   double prim_thr;
   double schwarz_thr;
+  int mode;          // kernel variant: 0 thread per quartet, 1 warp-cooperative, 2/3: 8/32 lanes per quartet
+  int natoms;        // gradient rows; accumulated per block in shared memory when gsmem
+  int gsmem;
+  int* next_task;    // work counter (zeroed before the launch)
 };
 
 struct OneEArgs {
@@ -130,6 +157,8 @@ cudaError_t launch_fock(const double* H, const double* Jt, const double* Kt, con
 cudaError_t launch_boys_batch(int m, int n, const double* T, double* F, cudaStream_t st);
 cudaError_t launch_rys_batch(int nr, int n, const double* T, double* R, double* W, cudaStream_t st);
 cudaError_t launch_one_electron(const OneEArgs& a, cudaStream_t st);
+cudaError_t launch_shell_dmax(const double* D, const int* shell_off, const int* shell_l, int n_shells, int nbf,
+                              double* dmax, cudaStream_t st);
 cudaError_t launch_count_prim_quartets(const ShellPair* pairs, const PrimPair* pp, const int* ket_list,
                                        const QuartetTask* tasks, int ntasks, double thr,
                                        unsigned long long* out, cudaStream_t st);

@@ -1,7 +1,7 @@
 // Auxiliary kernels of the ERI engine: Schwarz bounds, density/J/K scaling
 // and symmetrisation, Fock assembly, batched Boys/Rys evaluation, and the
 // class dispatch of the quartet kernels (instantiated in eri_inst_*.cu).
-#include "eri_templates.cuh"
+#include "eri_launch.cuh"
 
 namespace iqcp {
 
@@ -100,6 +100,26 @@ cudaError_t launch_rys_batch(int nr, int n, const double* T, double* R, double* 
   return cudaGetLastError();
 }
 
+
+// max |D| over each shell-pair block (mixed-precision quartet bound)
+__global__ void shell_dmax_kernel(const double* __restrict__ D, const int* __restrict__ off,
+                                  const int* __restrict__ l, int ns, int nbf, double* __restrict__ out) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= ns * ns) return;
+  const int a = idx / ns, b = idx % ns;
+  const int na = ncart(l[a]), nb = ncart(l[b]);
+  double m = 0.0;
+  for (int i = 0; i < na; ++i)
+    for (int j = 0; j < nb; ++j) m = fmax(m, fabs(D[(long long)(off[a] + i) * nbf + off[b] + j]));
+  out[idx] = m;
+}
+
+cudaError_t launch_shell_dmax(const double* D, const int* shell_off, const int* shell_l, int n_shells, int nbf,
+                              double* dmax, cudaStream_t st) {
+  const int n = n_shells * n_shells;
+  shell_dmax_kernel<<<(n + 127) / 128, 128, 0, st>>>(D, shell_off, shell_l, n_shells, nbf, dmax);
+  return cudaGetLastError();
+}
 
 // Surviving primitive quartets (K_ij * K_kl >= thr) of a task range.
 __global__ void count_prim_quartets_kernel(const ShellPair* __restrict__ pairs, const PrimPair* __restrict__ pp,

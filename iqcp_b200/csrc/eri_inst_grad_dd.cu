@@ -1,5 +1,5 @@
 // Instantiation of the grad quartet kernels for bra class (dd|
-#include "eri_templates.cuh"
+#include "eri_launch.cuh"
 
 namespace iqcp {
 template cudaError_t launch_grad_bra<2, 2>(int, const GradArgs&, cudaStream_t);

@@ -1,5 +1,5 @@
 // Instantiation of the jk quartet kernels for bra class (ds|
-#include "eri_templates.cuh"
+#include "eri_launch.cuh"
 
 namespace iqcp {
 template cudaError_t launch_jk_bra<2, 0>(int, const JKArgs&, cudaStream_t);

@@ -1,0 +1,127 @@
+// Launchers for one bra class (LA, LB) against every ket class Y <= X.
+// Classes with many components use the warp-cooperative kernels
+// (eri_team.cuh); the small ones keep one quartet per thread.
+#pragma once
+#include "eri_team.cuh"
+
+namespace iqcp {
+
+
+template <typename K>
+inline cudaError_t set_smem(K kernel, size_t bytes) {
+  if (bytes <= 48 * 1024) return cudaSuccess;
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+// Persistent grid: as many 128-thread blocks as are resident at once (capped
+// by the work), each looping over tasks; per-block set-up (the staged Rys
+// table, the gradient accumulator) is then paid once per resident block.
+template <typename K>
+inline int persistent_blocks(K kernel, size_t smem, int ntasks) {
+  int per_sm = 0, dev = 0, sms = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 128, smem);
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int need = (ntasks + 3) / 4;
+  const int cap = (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
+  return need < cap ? need : cap;
+}
+
+#define IQCP_LAUNCH(KERNEL, SMEM, ARGS, ST)                                      \
+  do {                                                                           \
+    cudaError_t e_ = set_smem(KERNEL, SMEM);                                     \
+    if (e_ != cudaSuccess) return e_;                                            \
+    KERNEL<<<persistent_blocks(KERNEL, SMEM, (ARGS).ntasks), 128, SMEM, ST>>>(ARGS); \
+  } while (0)
+
+// mode: 0 one quartet per thread, 1 warp-cooperative (eri_team.cuh),
+// 2 / 3 eight / thirty-two lanes share one quartet's primitive quartets
+// (small classes only; larger classes fall back to mode 0)
+template <int LA, int LB, int LC, int LD>
+cudaError_t launch_jk_class(const JKArgs& a, cudaStream_t st) {
+  using C = Cls<LA, LB, LC, LD>;
+  const size_t tb = sizeof(double) * rys_tab_doubles<C::NR>();
+  if (a.mode == 1) {
+    const size_t bytes = sizeof(double) * 4 * TeamJK<LA, LB, LC, LD>::PER_WARP + tb;
+    if (a.K) IQCP_LAUNCH((jk_team_kernel<LA, LB, LC, LD, true>), bytes, a, st);
+    else IQCP_LAUNCH((jk_team_kernel<LA, LB, LC, LD, false>), bytes, a, st);
+  } else if (C::NCOMP <= 27 && (a.mode == 2 || a.mode == 3)) {
+    if constexpr (C::NCOMP <= 27) {
+      if (a.mode == 2) {
+        if (a.K) IQCP_LAUNCH((jk_kernel<LA, LB, LC, LD, 8, true>), tb, a, st);
+        else IQCP_LAUNCH((jk_kernel<LA, LB, LC, LD, 8, false>), tb, a, st);
+      } else {
+        if (a.K) IQCP_LAUNCH((jk_kernel<LA, LB, LC, LD, 32, true>), tb, a, st);
+        else IQCP_LAUNCH((jk_kernel<LA, LB, LC, LD, 32, false>), tb, a, st);
+      }
+    }
+  } else {
+    if (a.K) IQCP_LAUNCH((jk_kernel<LA, LB, LC, LD, 1, true>), tb, a, st);
+    else IQCP_LAUNCH((jk_kernel<LA, LB, LC, LD, 1, false>), tb, a, st);
+  }
+  return cudaGetLastError();
+}
+
+template <int LA, int LB, int LC, int LD>
+cudaError_t launch_grad_class(const GradArgs& a, cudaStream_t st) {
+  using C = Cls<LA, LB, LC, LD>;
+  constexpr int NRG = (LA + LB + LC + LD + 2) / 2 + 1;
+  const size_t gacc = a.gsmem ? sizeof(double) * 3 * a.natoms : 0;
+  const size_t tb = sizeof(double) * rys_tab_doubles<NRG>() + gacc;
+  if (a.mode == 1) {
+    const size_t bytes = sizeof(double) * 4 * TeamGrad<LA, LB, LC, LD>::PER_WARP + tb;
+    IQCP_LAUNCH((grad_team_kernel<LA, LB, LC, LD>), bytes, a, st);
+  } else if (C::NCOMP <= 36 && (a.mode == 2 || a.mode == 3)) {
+    if constexpr (C::NCOMP <= 36) {
+      if (a.mode == 2) IQCP_LAUNCH((grad_kernel<LA, LB, LC, LD, 8>), tb, a, st);
+      else IQCP_LAUNCH((grad_kernel<LA, LB, LC, LD, 32>), tb, a, st);
+    }
+  } else {
+    IQCP_LAUNCH((grad_kernel<LA, LB, LC, LD, 1>), tb, a, st);
+  }
+  return cudaGetLastError();
+}
+
+#define IQCP_KET_DISPATCH(X, Y, MACRO)                \
+  switch (Y) {                                        \
+    case 0: MACRO(0, 0); break;                       \
+    case 1: if (X >= 1) { MACRO(1, 0); } break;       \
+    case 2: if (X >= 2) { MACRO(1, 1); } break;       \
+    case 3: if (X >= 3) { MACRO(2, 0); } break;       \
+    case 4: if (X >= 4) { MACRO(2, 1); } break;       \
+    case 5: if (X >= 5) { MACRO(2, 2); } break;       \
+    default: return cudaErrorInvalidValue;            \
+  }
+
+template <int LA, int LB>
+cudaError_t launch_jk_bra(int Y, const JKArgs& a, cudaStream_t st) {
+  constexpr int X = pair_class(LA, LB);
+#define LJK(lc, ld) \
+  if constexpr (pair_class(lc, ld) <= X) { return launch_jk_class<LA, LB, lc, ld>(a, st); }
+  IQCP_KET_DISPATCH(X, Y, LJK)
+#undef LJK
+  return cudaErrorInvalidValue;
+}
+
+template <int LA, int LB>
+cudaError_t launch_store_bra(int Y, const StoreArgs& a, cudaStream_t st) {
+  constexpr int X = pair_class(LA, LB);
+  const int blocks = (a.ntasks + 3) / 4;
+#define LST(lc, ld) \
+  if constexpr (pair_class(lc, ld) <= X) { store_kernel<LA, LB, lc, ld><<<blocks, 128, 0, st>>>(a); }
+  IQCP_KET_DISPATCH(X, Y, LST)
+#undef LST
+  return cudaGetLastError();
+}
+
+template <int LA, int LB>
+cudaError_t launch_grad_bra(int Y, const GradArgs& a, cudaStream_t st) {
+  constexpr int X = pair_class(LA, LB);
+#define LGR(lc, ld) \
+  if constexpr (pair_class(lc, ld) <= X) { return launch_grad_class<LA, LB, lc, ld>(a, st); }
+  IQCP_KET_DISPATCH(X, Y, LGR)
+#undef LGR
+  return cudaErrorInvalidValue;
+}
+
+}  // namespace iqcp

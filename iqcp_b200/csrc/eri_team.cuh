@@ -1,0 +1,458 @@
+// Warp-cooperative quartet kernels for the larger angular-momentum classes.
+//
+// One warp evaluates one contracted shell quartet at a time (the 32 kets of its
+// task one after another).  Per surviving primitive quartet:
+//   phase A  lanes 0 .. 3*NR-1 each take one (root, axis): the Rys root from
+//            the tables, the recurrence coefficients (rys_coefficients.rs:94),
+//            the 2D VRR (vrr_2d.rs:143) and the horizontal transfer to B and D
+//            (htr_4d.rs), written as one 1D table to shared memory;
+//   phase B  every lane accumulates its own components c = lane + 32 m of the
+//            block, sum over roots of Ix * Iy * Iz, from packed per-component
+//            table offsets held in registers.
+// The contracted block is then staged in shared memory and digested into J/K
+// (8-fold symmetry, degeneracy factors) with one atomic per output element, or
+// for gradients contracted with the D x D weights per primitive quartet.
+// Numerics are those of the thread-per-quartet kernels (eri_templates.cuh).
+#pragma once
+#include "eri_templates.cuh"
+
+namespace iqcp {
+
+// Rule for one root r of an N-point rule (phase A lanes each need one root).
+// (table staged in shared memory at s)
+template <int N>
+__device__ __forceinline__ void rys_rule_one(double T, int r, const double* s, double* t2, double* w) {
+  constexpr int NI = rys_nint(N);
+  if (T >= double(NI)) {
+    const int base = (N * (N - 1)) / 2;
+    *t2 = __ldg(kRysAsymRoot + base + r) / T;
+    *w = __ldg(kRysAsymWeight + base + r) / sqrt(T);
+    return;
+  }
+  const int k = int(T);
+  const double x2 = 2.0 * (2.0 * (T - double(k)) - 1.0);
+  const double* c = s + k * (2 * N * (RYS_TAB_DEG + 1));
+  *t2 = cheb_clenshaw_s(c + r * (RYS_TAB_DEG + 1), x2);
+  *w = cheb_clenshaw_s(c + (N + r) * (RYS_TAB_DEG + 1), x2);
+}
+
+// Shared-memory footprint (doubles) of one warp of the J/K team kernel
+template <int LA, int LB, int LC, int LD>
+struct TeamJK {
+  using C = Cls<LA, LB, LC, LD>;
+  static constexpr int TAB = C::NR * 3 * C::TSZ;
+  static constexpr int BLK = C::NCOMP;
+  static constexpr int WORK = TAB > BLK ? TAB : BLK;
+  static constexpr int DB = C::NA * C::NB + C::NC * C::ND + C::NB * C::ND + C::NA * C::ND + C::NB * C::NC +
+                            C::NA * C::NC;
+  static constexpr int PER_WARP = WORK + DB;
+  static constexpr int CPL = (C::NCOMP + 31) / 32;
+};
+
+// One contracted quartet: phases A and B over all surviving primitive
+// quartets, accumulating this lane's components into acc (FP64).  R is the
+// quadrature type: double, or float for the mixed form (roots, weights and
+// recurrence coefficients are formed in FP64 and rounded once).
+template <typename R, int LA, int LB, int LC, int LD>
+__device__ __forceinline__ void team_prim_loop(const JKArgs& args, const ShellPair& bp, const ShellPair& kp,
+                                               const double* AB, const double* CD, const int* offs, double* acc,
+                                               R* tab, int lane, const double* rtab) {
+  using C = Cls<LA, LB, LC, LD>;
+  constexpr int NR = C::NR, TSZ = C::TSZ, CPL = TeamJK<LA, LB, LC, LD>::CPL;
+  for (int i = 0; i < bp.np; ++i) {
+    const PrimPair pb = load_pp(args.pp + bp.pstart + i);
+    for (int j = 0; j < kp.np; ++j) {
+      const PrimPair pk = load_pp(args.pp + kp.pstart + j);
+      if (pb.K * pk.K < args.prim_thr) continue;
+      if (lane < 3 * NR) {
+        const int r = lane / 3, ax = lane - 3 * r;
+        const double p = pb.p, q = pk.p, s = p + q;
+        const double PQ[3] = {pb.P[0] - pk.P[0], pb.P[1] - pk.P[1], pb.P[2] - pk.P[2]};
+        const double inv_s = 1.0 / s;
+        const double rho = p * q * inv_s;
+        const double T = rho * (PQ[0] * PQ[0] + PQ[1] * PQ[1] + PQ[2] * PQ[2]);
+        double t2, wr;
+        rys_rule_one<NR>(T, r, rtab, &t2, &wr);
+        const double b00 = 0.5 * t2 * inv_s, h = 0.5 - 0.5 * t2;
+        const double b10 = fma(h, pb.inv_p, b00), b01 = fma(h, pk.inv_p, b00);
+        const double pa = pb.P[ax] - bp.A[ax], qc = pk.P[ax] - kp.A[ax];
+        const double g00 = ax == 2 ? wr * kTwoPi52 * pb.cK * pk.cK * pb.inv_p * pk.inv_p * inv_s * sqrt(s) : 1.0;
+        axis_table<R, C::NBRA, C::NKET, LA, LB, LC, LD>(
+            R(pa - t2 * q * inv_s * PQ[ax]), R(qc + t2 * p * inv_s * PQ[ax]), R(b00), R(b10), R(b01), R(AB[ax]),
+            R(CD[ax]), R(g00), tab + (r * 3 + ax) * TSZ);
+      }
+      __syncwarp();
+#pragma unroll
+      for (int m = 0; m < CPL; ++m) {
+        const int o = offs[m];
+        const int ox = o & 0xff, oy = (o >> 8) & 0xff, oz = (o >> 16) & 0xff;
+        R sum = R(0);
+#pragma unroll
+        for (int r = 0; r < NR; ++r) {
+          const R* t = tab + r * 3 * TSZ;
+          sum = fma(t[ox] * t[oy], t[oz], sum);
+        }
+        acc[m] += double(sum);
+      }
+      __syncwarp();
+    }
+  }
+}
+
+template <int LA, int LB, int LC, int LD, bool DO_K>
+__global__ void __launch_bounds__(128) jk_team_kernel(JKArgs args) {
+  using C = Cls<LA, LB, LC, LD>;
+  using TM = TeamJK<LA, LB, LC, LD>;
+  constexpr int NR = C::NR, TSZ = C::TSZ, CPL = TM::CPL;
+  extern __shared__ double smem[];
+  double* rtab = smem;
+  rys_stage_table<NR>(rtab);
+  __syncthreads();
+  const int wib = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  double* work = smem + rys_tab_doubles<NR>() + wib * TM::PER_WARP;
+  double* Dab = work + TM::WORK;
+  double* Dcd = Dab + C::NA * C::NB;
+  double* Dbd = Dcd + C::NC * C::ND;
+  double* Dad = Dbd + C::NB * C::ND;
+  double* Dbc = Dad + C::NA * C::ND;
+  double* Dac = Dbc + C::NB * C::NC;
+
+  // packed table offsets of this lane's components: x | y << 8 | z << 16
+  int offs[CPL];
+#pragma unroll
+  for (int m = 0; m < CPL; ++m) {
+    int comp = lane + 32 * m;
+    if (comp >= C::NCOMP) comp = 0;
+    const int d = comp % C::ND, c = (comp / C::ND) % C::NC, b = (comp / (C::ND * C::NC)) % C::NB,
+              a = comp / (C::ND * C::NC * C::NB);
+    int o = 0;
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax)
+      o |= (ax * TSZ + C::tidx(cart_pow(LA, a, ax), cart_pow(LB, b, ax), cart_pow(LC, c, ax),
+                               cart_pow(LD, d, ax))) << (8 * ax);
+    offs[m] = o;
+  }
+
+  for (int warp = next_task(args.next_task, lane); warp < args.ntasks; warp = next_task(args.next_task, lane)) {
+  const QuartetTask task = args.tasks[warp];
+  const ShellPair bp = args.pairs[task.bra];
+  const int n = args.nbf;
+  const double* __restrict__ D = args.D;
+  const double AB[3] = {bp.A[0] - bp.B[0], bp.A[1] - bp.B[1], bp.A[2] - bp.B[2]};
+  __syncwarp();
+  for (int i = lane; i < C::NA * C::NB; i += 32)
+    Dab[i] = __ldg(D + (bp.oa + i / C::NB) * n + bp.ob + i % C::NB);
+
+  for (int kk = 0; kk < task.nket; ++kk) {
+    const int kpos = task.ket0 + kk;
+    const ShellPair kp = args.pairs[__ldg(args.ket_list + kpos)];
+    const double CD[3] = {kp.A[0] - kp.B[0], kp.A[1] - kp.B[1], kp.A[2] - kp.B[2]};
+    double acc[CPL];
+#pragma unroll
+    for (int m = 0; m < CPL; ++m) acc[m] = 0.0;
+    bool f32 = false;
+    if (args.dmax_shell) {
+      // mixed precision: Schwarz bound x largest |D| this quartet digests with
+      const int ns = args.n_shells;
+      const double* dm = args.dmax_shell;
+      double dmax = fmax(fmax(dm[bp.sa * ns + bp.sb], dm[kp.sa * ns + kp.sb]),
+                         fmax(fmax(dm[bp.sa * ns + kp.sa], dm[bp.sa * ns + kp.sb]),
+                              fmax(dm[bp.sb * ns + kp.sa], dm[bp.sb * ns + kp.sb])));
+      f32 = bp.Q * kp.Q * dmax < args.mixed_cutoff;
+    }
+    if (f32) {
+      team_prim_loop<float, LA, LB, LC, LD>(args, bp, kp, AB, CD, offs, acc, reinterpret_cast<float*>(work), lane, rtab);
+      if (lane == 0 && args.fp32_count) atomicAdd(args.fp32_count, 1ull);
+    } else {
+      team_prim_loop<double, LA, LB, LC, LD>(args, bp, kp, AB, CD, offs, acc, work, lane, rtab);
+    }
+    // ---- digestion ----
+    double f = 1.0;
+    if (bp.sa == bp.sb) f *= 0.5;
+    if (kp.sa == kp.sb) f *= 0.5;
+    if (task.diag && kpos == task.bra_pos) f *= 0.5;
+#pragma unroll
+    for (int m = 0; m < CPL; ++m) {
+      const int comp = lane + 32 * m;
+      if (comp < C::NCOMP) work[comp] = f * acc[m];
+    }
+    for (int i = lane; i < C::NC * C::ND; i += 32) Dcd[i] = __ldg(D + (kp.oa + i / C::ND) * n + kp.ob + i % C::ND);
+    if (DO_K) {
+      for (int i = lane; i < C::NB * C::ND; i += 32) Dbd[i] = __ldg(D + (bp.ob + i / C::ND) * n + kp.ob + i % C::ND);
+      for (int i = lane; i < C::NA * C::ND; i += 32) Dad[i] = __ldg(D + (bp.oa + i / C::ND) * n + kp.ob + i % C::ND);
+      for (int i = lane; i < C::NB * C::NC; i += 32) Dbc[i] = __ldg(D + (bp.ob + i / C::NC) * n + kp.oa + i % C::NC);
+      for (int i = lane; i < C::NA * C::NC; i += 32) Dac[i] = __ldg(D + (bp.oa + i / C::NC) * n + kp.oa + i % C::NC);
+    }
+    __syncwarp();
+    // J~_ab += 2 sum_cd I D_cd
+    for (int ab = lane; ab < C::NA * C::NB; ab += 32) {
+      double v = 0.0;
+#pragma unroll
+      for (int cd = 0; cd < C::NC * C::ND; ++cd) v = fma(work[ab * C::NC * C::ND + cd], Dcd[cd], v);
+      atomicAdd(args.J + (bp.oa + ab / C::NB) * n + bp.ob + ab % C::NB, 2.0 * v);
+    }
+    // J~_cd += 2 sum_ab I D_ab
+    for (int cd = lane; cd < C::NC * C::ND; cd += 32) {
+      double v = 0.0;
+#pragma unroll
+      for (int ab = 0; ab < C::NA * C::NB; ++ab) v = fma(work[ab * C::NC * C::ND + cd], Dab[ab], v);
+      atomicAdd(args.J + (kp.oa + cd / C::ND) * n + kp.ob + cd % C::ND, 2.0 * v);
+    }
+    if (DO_K) {
+      // K~_ac += sum_bd I D_bd
+      for (int x = lane; x < C::NA * C::NC; x += 32) {
+        const int a = x / C::NC, c = x % C::NC;
+        double v = 0.0;
+#pragma unroll
+        for (int b = 0; b < C::NB; ++b)
+#pragma unroll
+          for (int d = 0; d < C::ND; ++d)
+            v = fma(work[((a * C::NB + b) * C::NC + c) * C::ND + d], Dbd[b * C::ND + d], v);
+        atomicAdd(args.K + (bp.oa + a) * n + kp.oa + c, v);
+      }
+      // K~_bc += sum_ad I D_ad
+      for (int x = lane; x < C::NB * C::NC; x += 32) {
+        const int b = x / C::NC, c = x % C::NC;
+        double v = 0.0;
+#pragma unroll
+        for (int a = 0; a < C::NA; ++a)
+#pragma unroll
+          for (int d = 0; d < C::ND; ++d)
+            v = fma(work[((a * C::NB + b) * C::NC + c) * C::ND + d], Dad[a * C::ND + d], v);
+        atomicAdd(args.K + (bp.ob + b) * n + kp.oa + c, v);
+      }
+      // K~_ad += sum_bc I D_bc
+      for (int x = lane; x < C::NA * C::ND; x += 32) {
+        const int a = x / C::ND, d = x % C::ND;
+        double v = 0.0;
+#pragma unroll
+        for (int b = 0; b < C::NB; ++b)
+#pragma unroll
+          for (int c = 0; c < C::NC; ++c)
+            v = fma(work[((a * C::NB + b) * C::NC + c) * C::ND + d], Dbc[b * C::NC + c], v);
+        atomicAdd(args.K + (bp.oa + a) * n + kp.ob + d, v);
+      }
+      // K~_bd += sum_ac I D_ac
+      for (int x = lane; x < C::NB * C::ND; x += 32) {
+        const int b = x / C::ND, d = x % C::ND;
+        double v = 0.0;
+#pragma unroll
+        for (int a = 0; a < C::NA; ++a)
+#pragma unroll
+          for (int c = 0; c < C::NC; ++c)
+            v = fma(work[((a * C::NB + b) * C::NC + c) * C::ND + d], Dac[a * C::NC + c], v);
+        atomicAdd(args.K + (bp.ob + b) * n + kp.ob + d, v);
+      }
+    }
+    __syncwarp();
+  }
+  }  // task loop
+}
+
+// ---------------------------------------------------------------------------
+// Gradient team kernel.  Tables are extended by one on A, B and C (the D
+// derivative follows from translational invariance, dD = -(dA + dB + dC)),
+// with one more root than the energy (gradient.rs / eri/mod.rs:2146-2149).
+template <int LA, int LB, int LC, int LD>
+struct TeamGrad {
+  using C = Cls<LA, LB, LC, LD>;
+  static constexpr int EA = LA + 1, EB = LB + 1, EC = LC + 1, ED = LD;
+  static constexpr int NR = (LA + LB + LC + LD + 2) / 2 + 1;
+  static constexpr int TSZ = (EA + 1) * (EB + 1) * (EC + 1) * (ED + 1);
+  static constexpr int SA = (EB + 1) * (EC + 1) * (ED + 1), SB = (EC + 1) * (ED + 1), SC = ED + 1;
+  static constexpr int TAB = NR * 3 * TSZ;
+  static constexpr int DBLK = C::NA * C::NB + C::NC * C::ND + C::NA * C::NC + C::NB * C::ND + C::NA * C::ND +
+                              C::NB * C::NC;
+  static constexpr int PER_WARP = TAB + DBLK;
+  static constexpr int CPL = (C::NCOMP + 31) / 32;
+  __host__ __device__ static constexpr int eidx(int a, int b, int c, int d) {
+    return ((a * (EB + 1) + b) * (EC + 1) + c) * (ED + 1) + d;
+  }
+};
+
+template <int LA, int LB, int LC, int LD>
+__global__ void __launch_bounds__(128) grad_team_kernel(GradArgs args) {
+  using C = Cls<LA, LB, LC, LD>;
+  using TG = TeamGrad<LA, LB, LC, LD>;
+  constexpr int NR = TG::NR, TSZ = TG::TSZ, CPL = TG::CPL;
+  extern __shared__ double smem[];
+  double* rtab = smem;
+  rys_stage_table<NR>(rtab);
+  __syncthreads();
+  const int wib = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  double* tab = smem + rys_tab_doubles<NR>() + wib * TG::PER_WARP;
+  double* gacc = smem + rys_tab_doubles<NR>() + 4 * TG::PER_WARP;
+  if (args.gsmem)
+    for (int i = threadIdx.x; i < 3 * args.natoms; i += blockDim.x) gacc[i] = 0.0;
+  __syncthreads();
+  double* gout = args.gsmem ? gacc : args.grad;
+  double* Dab = tab + TG::TAB;
+  double* Dcd = Dab + C::NA * C::NB;
+  double* Dac = Dcd + C::NC * C::ND;
+  double* Dbd = Dac + C::NA * C::NC;
+  double* Dad = Dbd + C::NB * C::ND;
+  double* Dbc = Dad + C::NA * C::ND;
+
+  // packed per-component data: table offsets (3 x 8 bits) and A/B/C powers (9 x 2 bits)
+  int offs[CPL], pows[CPL];
+#pragma unroll
+  for (int m = 0; m < CPL; ++m) {
+    int comp = lane + 32 * m;
+    if (comp >= C::NCOMP) comp = 0;
+    const int d = comp % C::ND, c = (comp / C::ND) % C::NC, b = (comp / (C::ND * C::NC)) % C::NB,
+              a = comp / (C::ND * C::NC * C::NB);
+    int o = 0, pw = 0;
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+      const int ia = cart_pow(LA, a, ax), ib = cart_pow(LB, b, ax), ic = cart_pow(LC, c, ax),
+                id = cart_pow(LD, d, ax);
+      o |= (ax * TSZ + TG::eidx(ia, ib, ic, id)) << (10 * ax);
+      pw |= (ia | (ib << 2) | (ic << 4)) << (6 * ax);
+    }
+    offs[m] = o;
+    pows[m] = pw;
+  }
+
+  for (int warp = next_task(args.next_task, lane); warp < args.ntasks; warp = next_task(args.next_task, lane)) {
+  const QuartetTask task = args.tasks[warp];
+  const ShellPair bp = args.pairs[task.bra];
+  const int n = args.nbf;
+  const double* __restrict__ D = args.D;
+  const double AB[3] = {bp.A[0] - bp.B[0], bp.A[1] - bp.B[1], bp.A[2] - bp.B[2]};
+  __syncwarp();
+  for (int i = lane; i < C::NA * C::NB; i += 32)
+    Dab[i] = __ldg(D + (bp.oa + i / C::NB) * n + bp.ob + i % C::NB);
+  const bool ij_same = bp.sa == bp.sb;
+  const double xs = args.xscale;
+
+  for (int kk = 0; kk < task.nket; ++kk) {
+    const int kpos = task.ket0 + kk;
+    const ShellPair kp = args.pairs[__ldg(args.ket_list + kpos)];
+    // the reference skips when the Schwarz bound of its bra pair (the larger
+    // composite index) is below threshold (gradient.rs:1457-1460)
+    const double qref = bp.comp >= kp.comp ? bp.Q : kp.Q;
+    if (qref < args.schwarz_thr) continue;
+    const bool kl_same = kp.sa == kp.sb;
+    const bool bk_same = task.diag && kpos == task.bra_pos;
+    for (int i = lane; i < C::NC * C::ND; i += 32) Dcd[i] = __ldg(D + (kp.oa + i / C::ND) * n + kp.ob + i % C::ND);
+    for (int i = lane; i < C::NA * C::NC; i += 32) Dac[i] = __ldg(D + (bp.oa + i / C::NC) * n + kp.oa + i % C::NC);
+    for (int i = lane; i < C::NB * C::ND; i += 32) Dbd[i] = __ldg(D + (bp.ob + i / C::ND) * n + kp.ob + i % C::ND);
+    for (int i = lane; i < C::NA * C::ND; i += 32) Dad[i] = __ldg(D + (bp.oa + i / C::ND) * n + kp.ob + i % C::ND);
+    for (int i = lane; i < C::NB * C::NC; i += 32) Dbc[i] = __ldg(D + (bp.ob + i / C::NC) * n + kp.oa + i % C::NC);
+    __syncwarp();
+    // D x D weights of this lane's components (compute_symmetry_weight, gradient.rs:1570-1640)
+    double W[CPL];
+#pragma unroll
+    for (int m = 0; m < CPL; ++m) {
+      const int comp = lane + 32 * m;
+      double t = 0.0;
+      if (comp < C::NCOMP) {
+        const int d = comp % C::ND, c = (comp / C::ND) % C::NC, b = (comp / (C::ND * C::NC)) % C::NB,
+                  a = comp / (C::ND * C::NC * C::NB);
+        const double dab = Dab[a * C::NB + b], dcd = Dcd[c * C::ND + d];
+        const double dac = Dac[a * C::NC + c], dbd = Dbd[b * C::ND + d];
+        const double dad = Dad[a * C::ND + d], dbc = Dbc[b * C::NC + c];
+        // w(p,q,r,s) = 1/2 D_pq D_rs - xs D_pr D_qs over the distinct permutations
+        t = 0.5 * dab * dcd - xs * dac * dbd;                       // (ij|kl)
+        if (!ij_same) t += 0.5 * dab * dcd - xs * dbc * dad;        // (ji|kl)
+        if (!kl_same) t += 0.5 * dab * dcd - xs * dad * dbc;        // (ij|lk)
+        if (!ij_same && !kl_same) t += 0.5 * dab * dcd - xs * dbd * dac;  // (ji|lk)
+        if (!bk_same) {
+          t += 0.5 * dcd * dab - xs * dac * dbd;                     // (kl|ij)
+          if (!kl_same) t += 0.5 * dcd * dab - xs * dad * dbc;       // (lk|ij)
+          if (!ij_same) t += 0.5 * dcd * dab - xs * dbc * dad;       // (kl|ji)
+          if (!ij_same && !kl_same) t += 0.5 * dcd * dab - xs * dbd * dac;  // (lk|ji)
+        }
+        const double angp = ang_factor(LA, a) * ang_factor(LB, b) * ang_factor(LC, c) * ang_factor(LD, d);
+        if (fabs(t / angp) < 1e-15) t = 0.0;  // |w| < 1e-15 skip on the reference weight
+      }
+      W[m] = t;
+    }
+    double g[9];
+#pragma unroll
+    for (int x = 0; x < 9; ++x) g[x] = 0.0;
+    const double CD[3] = {kp.A[0] - kp.B[0], kp.A[1] - kp.B[1], kp.A[2] - kp.B[2]};
+    for (int i = 0; i < bp.np; ++i) {
+      const PrimPair pb = load_pp(args.pp + bp.pstart + i);
+      for (int j = 0; j < kp.np; ++j) {
+        const PrimPair pk = load_pp(args.pp + kp.pstart + j);
+        if (pb.K * pk.K < args.prim_thr) continue;
+        __syncwarp();
+        if (lane < 3 * NR) {
+          const int r = lane / 3, ax = lane - 3 * r;
+          const double p = pb.p, q = pk.p, s = p + q;
+          const double PQ[3] = {pb.P[0] - pk.P[0], pb.P[1] - pk.P[1], pb.P[2] - pk.P[2]};
+          const double inv_s = 1.0 / s;
+        const double rho = p * q * inv_s;
+          const double T = rho * (PQ[0] * PQ[0] + PQ[1] * PQ[1] + PQ[2] * PQ[2]);
+          double t2, wr;
+          rys_rule_one<NR>(T, r, rtab, &t2, &wr);
+          const double b00 = 0.5 * t2 * inv_s, h = 0.5 - 0.5 * t2;
+          const double b10 = fma(h, pb.inv_p, b00), b01 = fma(h, pk.inv_p, b00);
+          const double pa = pb.P[ax] - bp.A[ax], qc = pk.P[ax] - kp.A[ax];
+          const double g00 = ax == 2 ? wr * kTwoPi52 * pb.cK * pk.cK * pb.inv_p * pk.inv_p * inv_s * sqrt(s) : 1.0;
+          axis_table<double, LA + LB + 1, LC + LD + 1, TG::EA, TG::EB, TG::EC, TG::ED>(
+              pa - t2 * q * inv_s * PQ[ax], qc + t2 * p * inv_s * PQ[ax], b00, b10, b01, AB[ax], CD[ax], g00,
+              tab + (r * 3 + ax) * TSZ);
+        }
+        __syncwarp();
+        const double e2[3] = {2.0 * pb.aa, 2.0 * (pb.p - pb.aa), 2.0 * pk.aa};
+        const int str[3] = {TG::SA, TG::SB, TG::SC};
+#pragma unroll
+        for (int m = 0; m < CPL; ++m) {
+          const double w = W[m];
+          if (w == 0.0) continue;
+          const int o = offs[m], pw = pows[m];
+#pragma unroll
+          for (int r = 0; r < NR; ++r) {
+            const double* t = tab + r * 3 * TSZ;
+            int ox[3];
+            double reg[3];
+#pragma unroll
+            for (int ax = 0; ax < 3; ++ax) {
+              ox[ax] = (o >> (10 * ax)) & 0x3ff;
+              reg[ax] = t[ox[ax]];
+            }
+            const double wyz = w * reg[1] * reg[2], wxz = w * reg[0] * reg[2], wxy = w * reg[0] * reg[1];
+            const double wo[3] = {wyz, wxz, wxy};
+#pragma unroll
+            for (int ax = 0; ax < 3; ++ax) {
+#pragma unroll
+              for (int cen = 0; cen < 3; ++cen) {
+                const int pcen = (pw >> (6 * ax + 2 * cen)) & 3;
+                const double up = t[ox[ax] + str[cen]];
+                // power 0 has no lowered term; the index is clamped so no load leaves the table
+                const double dn = double(pcen) * t[pcen ? ox[ax] - str[cen] : ox[ax]];
+                g[3 * cen + ax] = fma(wo[ax], e2[cen] * up - dn, g[3 * cen + ax]);
+              }
+            }
+          }
+        }
+      }
+    }
+    // warp reduction of the nine derivatives, then atomics (D by invariance)
+#pragma unroll
+    for (int x = 0; x < 9; ++x) g[x] = warp_sum(g[x]);
+    if (lane == 0) {
+      double* gr = gout;
+#pragma unroll
+      for (int ax = 0; ax < 3; ++ax) {
+        atomicAdd(gr + 3 * bp.atom_a + ax, g[ax]);
+        atomicAdd(gr + 3 * bp.atom_b + ax, g[3 + ax]);
+        atomicAdd(gr + 3 * kp.atom_a + ax, g[6 + ax]);
+        atomicAdd(gr + 3 * kp.atom_b + ax, -(g[ax] + g[3 + ax] + g[6 + ax]));
+      }
+    }
+    __syncwarp();
+  }
+  }  // task loop
+  if (args.gsmem) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < 3 * args.natoms; i += blockDim.x)
+      if (gacc[i] != 0.0) atomicAdd(args.grad + i, gacc[i]);
+  }
+}
+
+}  // namespace iqcp

@@ -107,43 +107,49 @@ __device__ __forceinline__ PrimPair load_pp(const PrimPair* __restrict__ p) {
   const double2* s = reinterpret_cast<const double2*>(p);
   const double2 v0 = __ldg(s), v1 = __ldg(s + 1), v2 = __ldg(s + 2), v3 = __ldg(s + 3);
   r.p = v0.x; r.P[0] = v0.y; r.P[1] = v1.x; r.P[2] = v1.y;
-  r.K = v2.x; r.cK = v2.y; r.aa = v3.x; r.ab = v3.y;
+  r.K = v2.x; r.cK = v2.y; r.aa = v3.x; r.inv_p = v3.y;
   return r;
 }
 
 // Contracted (radially normalised) quartet (ab|cd) into acc[NCOMP], FP64.
+// Primitive quartets are visited as items it = i * np_ket + j, starting at
+// `first` with step `stride`, so that `stride` lanes can share one quartet.
 template <int LA, int LB, int LC, int LD>
 __device__ __forceinline__ void quartet_fp64(const ShellPair& bp, const ShellPair& kp,
                                              const PrimPair* __restrict__ pp, double thr,
-                                             double* __restrict__ acc) {
+                                             double* __restrict__ acc, int first = 0, int stride = 1,
+                                             const double* rtab = nullptr) {
   using C = Cls<LA, LB, LC, LD>;
 #pragma unroll
   for (int i = 0; i < C::NCOMP; ++i) acc[i] = 0.0;
   const double AB[3] = {bp.A[0] - bp.B[0], bp.A[1] - bp.B[1], bp.A[2] - bp.B[2]};
   const double CD[3] = {kp.A[0] - kp.B[0], kp.A[1] - kp.B[1], kp.A[2] - kp.B[2]};
-  for (int i = 0; i < bp.np; ++i) {
+  const int nitems = bp.np * kp.np;
+  for (int it = first; it < nitems; it += stride) {
+    const int i = it / kp.np, j = it - i * kp.np;
     const PrimPair b = load_pp(pp + bp.pstart + i);
-    for (int j = 0; j < kp.np; ++j) {
+    {
       const PrimPair k = load_pp(pp + kp.pstart + j);
       if (b.K * k.K < thr) continue;
       const double p = b.p, q = k.p, s = p + q;
       const double PQ[3] = {b.P[0] - k.P[0], b.P[1] - k.P[1], b.P[2] - k.P[2]};
-      const double rho = p * q / s;
+      const double inv_s = 1.0 / s;
+        const double rho = p * q * inv_s;
       const double T = rho * (PQ[0] * PQ[0] + PQ[1] * PQ[1] + PQ[2] * PQ[2]);
-      const double pref = kTwoPi52 * b.cK * k.cK / (p * q * sqrt(s));
+      const double pref = kTwoPi52 * b.cK * k.cK * b.inv_p * k.inv_p * inv_s * sqrt(s);
       double rt[C::NR], wt[C::NR];
-      rys_rule<C::NR>(T, rt, wt);
+      if (rtab) rys_rule_tab<C::NR>(T, rtab, rt, wt);
+      else rys_rule<C::NR>(T, rt, wt);
       const double PA[3] = {b.P[0] - bp.A[0], b.P[1] - bp.A[1], b.P[2] - bp.A[2]};
       const double QC[3] = {k.P[0] - kp.A[0], k.P[1] - kp.A[1], k.P[2] - kp.A[2]};
 #pragma unroll
       for (int r = 0; r < C::NR; ++r) {
         const double t2 = rt[r];
-        const double u = t2 < 1.0 - 1e-15 ? t2 / (1.0 - t2) : 1e15;
-        const double u2 = rho * u;
-        const double tmp4 = 0.5 / (u2 * s + p * q);
-        const double tmp5 = u2 * tmp4;
-        const double b00 = tmp5, b10 = tmp5 + tmp4 * q, b01 = tmp5 + tmp4 * p;
-        const double f2 = 2.0 * tmp5 * q, f3 = 2.0 * tmp5 * p;
+        // rys_coefficients.rs:94-180 with u2 (p+q) + pq = pq / (1 - t^2):
+        // tmp5 = t^2 / (2(p+q)), tmp4 q = (1 - t^2) / (2p), tmp4 p = (1 - t^2) / (2q)
+        const double b00 = 0.5 * t2 * inv_s, h = 0.5 - 0.5 * t2;
+        const double b10 = fma(h, b.inv_p, b00), b01 = fma(h, k.inv_p, b00);
+        const double f2 = t2 * q * inv_s, f3 = t2 * p * inv_s;
         double Ix[C::TSZ], Iy[C::TSZ], Iz[C::TSZ];
         axis_table<double, C::NBRA, C::NKET, LA, LB, LC, LD>(
             PA[0] - f2 * PQ[0], QC[0] + f3 * PQ[0], b00, b10, b01, AB[0], CD[0], 1.0, Ix);
@@ -179,119 +185,141 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
-template <int LA, int LB, int LC, int LD, bool DO_K>
+// Quartet kernel with G lanes per contracted quartet (G = 1, 8 or 32): the 32/G
+// groups of a warp take consecutive kets of the task; the G lanes of a group
+// split the quartet's primitive quartets and combine their partial blocks with
+// a segmented shuffle reduction; lane 0 of each group digests the block.
+template <int G>
+__device__ __forceinline__ double group_sum(double v) {
+#pragma unroll
+  for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+template <int LA, int LB, int LC, int LD, int G, bool DO_K>
 __global__ void __launch_bounds__(128) jk_kernel(JKArgs args) {
   using C = Cls<LA, LB, LC, LD>;
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  constexpr int NG = 32 / G;
+  extern __shared__ double rtab[];
+  rys_stage_table<C::NR>(rtab);
+  __syncthreads();
   const int lane = threadIdx.x & 31;
-  if (warp >= args.ntasks) return;  // uniform per warp
+  for (int warp = next_task(args.next_task, lane); warp < args.ntasks; warp = next_task(args.next_task, lane)) {
   const QuartetTask task = args.tasks[warp];
   const ShellPair bp = args.pairs[task.bra];
-  const bool active = lane < task.nket;
-  double acc[C::NCOMP];
-  double f = 0.0;
-  ShellPair kp = bp;
-  if (active) {
-    const int kpos = task.ket0 + lane;
-    kp = args.pairs[__ldg(args.ket_list + kpos)];
-    quartet_fp64<LA, LB, LC, LD>(bp, kp, args.pp, args.prim_thr, acc);
-    f = 1.0;
-    if (bp.sa == bp.sb) f *= 0.5;
-    if (kp.sa == kp.sb) f *= 0.5;
-    if (task.diag && kpos == task.bra_pos) f *= 0.5;
-  } else {
-#pragma unroll
-    for (int i = 0; i < C::NCOMP; ++i) acc[i] = 0.0;
-  }
+  const int grp = lane / G, sub = lane - grp * G;
   const int n = args.nbf;
   const double* __restrict__ D = args.D;
-  // J~_ab += 2f sum_cd (ab|cd) D_cd  -- same bra on every lane: warp reduction
+  for (int kbase = 0; kbase < task.nket; kbase += NG) {
+    const int kk = kbase + grp;
+    const bool active = kk < task.nket;
+    double acc[C::NCOMP];
+    double f = 0.0;
+    ShellPair kp = bp;
+    if (active) {
+      const int kpos = task.ket0 + kk;
+      kp = args.pairs[__ldg(args.ket_list + kpos)];
+      quartet_fp64<LA, LB, LC, LD>(bp, kp, args.pp, args.prim_thr, acc, sub, G, rtab);
+      f = 1.0;
+      if (bp.sa == bp.sb) f *= 0.5;
+      if (kp.sa == kp.sb) f *= 0.5;
+      if (task.diag && kpos == task.bra_pos) f *= 0.5;
+    } else {
 #pragma unroll
-  for (int a = 0; a < C::NA; ++a)
-#pragma unroll
-    for (int b = 0; b < C::NB; ++b) {
-      double v = 0.0;
-      if (active) {
-#pragma unroll
-        for (int c = 0; c < C::NC; ++c)
-#pragma unroll
-          for (int d = 0; d < C::ND; ++d)
-            v = fma(acc[((a * C::NB + b) * C::NC + c) * C::ND + d],
-                    __ldg(D + (kp.oa + c) * n + kp.ob + d), v);
-        v *= 2.0 * f;
-      }
-      v = warp_sum(v);
-      if (lane == 0) atomicAdd(args.J + (bp.oa + a) * n + bp.ob + b, v);
+      for (int i = 0; i < C::NCOMP; ++i) acc[i] = 0.0;
     }
-  if (!active) return;
-  // J~_cd += 2f sum_ab (ab|cd) D_ab
-  {
-    double dab[C::NA * C::NB];
+    if (G > 1) {
+#pragma unroll
+      for (int i = 0; i < C::NCOMP; ++i) acc[i] = group_sum<G>(acc[i]);
+    }
+    const bool digest = active && sub == 0;
+    // J~_ab += 2f sum_cd (ab|cd) D_cd  -- same bra on every group: warp reduction
 #pragma unroll
     for (int a = 0; a < C::NA; ++a)
 #pragma unroll
-      for (int b = 0; b < C::NB; ++b) dab[a * C::NB + b] = __ldg(D + (bp.oa + a) * n + bp.ob + b);
+      for (int b = 0; b < C::NB; ++b) {
+        double v = 0.0;
+        if (digest) {
 #pragma unroll
-    for (int c = 0; c < C::NC; ++c)
+          for (int c = 0; c < C::NC; ++c)
+#pragma unroll
+            for (int d = 0; d < C::ND; ++d)
+              v = fma(acc[((a * C::NB + b) * C::NC + c) * C::ND + d], __ldg(D + (kp.oa + c) * n + kp.ob + d), v);
+          v *= 2.0 * f;
+        }
+        v = warp_sum(v);
+        if (lane == 0) atomicAdd(args.J + (bp.oa + a) * n + bp.ob + b, v);
+      }
+    if (!digest) continue;
+    // J~_cd += 2f sum_ab (ab|cd) D_ab
+    {
+      double dab[C::NA * C::NB];
+#pragma unroll
+      for (int a = 0; a < C::NA; ++a)
+#pragma unroll
+        for (int b = 0; b < C::NB; ++b) dab[a * C::NB + b] = __ldg(D + (bp.oa + a) * n + bp.ob + b);
+#pragma unroll
+      for (int c = 0; c < C::NC; ++c)
+#pragma unroll
+        for (int d = 0; d < C::ND; ++d) {
+          double v = 0.0;
+#pragma unroll
+          for (int ab = 0; ab < C::NA * C::NB; ++ab) v = fma(acc[(ab * C::NC + c) * C::ND + d], dab[ab], v);
+          atomicAdd(args.J + (kp.oa + c) * n + kp.ob + d, 2.0 * f * v);
+        }
+    }
+    if (!DO_K) continue;
+    // K~_ac += f sum_bd I D_bd ; K~_bc += f sum_ad I D_ad ; K~_ad += f sum_bc I D_bc ; K~_bd += f sum_ac I D_ac
+#pragma unroll
+    for (int a = 0; a < C::NA; ++a)
+#pragma unroll
+      for (int c = 0; c < C::NC; ++c) {
+        double v = 0.0;
+#pragma unroll
+        for (int b = 0; b < C::NB; ++b)
+#pragma unroll
+          for (int d = 0; d < C::ND; ++d)
+            v = fma(acc[((a * C::NB + b) * C::NC + c) * C::ND + d], __ldg(D + (bp.ob + b) * n + kp.ob + d), v);
+        atomicAdd(args.K + (bp.oa + a) * n + kp.oa + c, f * v);
+      }
+#pragma unroll
+    for (int b = 0; b < C::NB; ++b)
+#pragma unroll
+      for (int c = 0; c < C::NC; ++c) {
+        double v = 0.0;
+#pragma unroll
+        for (int a = 0; a < C::NA; ++a)
+#pragma unroll
+          for (int d = 0; d < C::ND; ++d)
+            v = fma(acc[((a * C::NB + b) * C::NC + c) * C::ND + d], __ldg(D + (bp.oa + a) * n + kp.ob + d), v);
+        atomicAdd(args.K + (bp.ob + b) * n + kp.oa + c, f * v);
+      }
+#pragma unroll
+    for (int a = 0; a < C::NA; ++a)
 #pragma unroll
       for (int d = 0; d < C::ND; ++d) {
         double v = 0.0;
 #pragma unroll
-        for (int ab = 0; ab < C::NA * C::NB; ++ab)
-          v = fma(acc[(ab * C::NC + c) * C::ND + d], dab[ab], v);
-        atomicAdd(args.J + (kp.oa + c) * n + kp.ob + d, 2.0 * f * v);
+        for (int b = 0; b < C::NB; ++b)
+#pragma unroll
+          for (int c = 0; c < C::NC; ++c)
+            v = fma(acc[((a * C::NB + b) * C::NC + c) * C::ND + d], __ldg(D + (bp.ob + b) * n + kp.oa + c), v);
+        atomicAdd(args.K + (bp.oa + a) * n + kp.ob + d, f * v);
+      }
+#pragma unroll
+    for (int b = 0; b < C::NB; ++b)
+#pragma unroll
+      for (int d = 0; d < C::ND; ++d) {
+        double v = 0.0;
+#pragma unroll
+        for (int a = 0; a < C::NA; ++a)
+#pragma unroll
+          for (int c = 0; c < C::NC; ++c)
+            v = fma(acc[((a * C::NB + b) * C::NC + c) * C::ND + d], __ldg(D + (bp.oa + a) * n + kp.oa + c), v);
+        atomicAdd(args.K + (bp.ob + b) * n + kp.ob + d, f * v);
       }
   }
-  if (!DO_K) return;
-  // K~_ac += f sum_bd I D_bd ; K~_bc += f sum_ad I D_ad ; K~_ad += f sum_bc I D_bc ; K~_bd += f sum_ac I D_ac
-#pragma unroll
-  for (int a = 0; a < C::NA; ++a)
-#pragma unroll
-    for (int c = 0; c < C::NC; ++c) {
-      double v = 0.0;
-#pragma unroll
-      for (int b = 0; b < C::NB; ++b)
-#pragma unroll
-        for (int d = 0; d < C::ND; ++d)
-          v = fma(acc[((a * C::NB + b) * C::NC + c) * C::ND + d], __ldg(D + (bp.ob + b) * n + kp.ob + d), v);
-      atomicAdd(args.K + (bp.oa + a) * n + kp.oa + c, f * v);
-    }
-#pragma unroll
-  for (int b = 0; b < C::NB; ++b)
-#pragma unroll
-    for (int c = 0; c < C::NC; ++c) {
-      double v = 0.0;
-#pragma unroll
-      for (int a = 0; a < C::NA; ++a)
-#pragma unroll
-        for (int d = 0; d < C::ND; ++d)
-          v = fma(acc[((a * C::NB + b) * C::NC + c) * C::ND + d], __ldg(D + (bp.oa + a) * n + kp.ob + d), v);
-      atomicAdd(args.K + (bp.ob + b) * n + kp.oa + c, f * v);
-    }
-#pragma unroll
-  for (int a = 0; a < C::NA; ++a)
-#pragma unroll
-    for (int d = 0; d < C::ND; ++d) {
-      double v = 0.0;
-#pragma unroll
-      for (int b = 0; b < C::NB; ++b)
-#pragma unroll
-        for (int c = 0; c < C::NC; ++c)
-          v = fma(acc[((a * C::NB + b) * C::NC + c) * C::ND + d], __ldg(D + (bp.ob + b) * n + kp.oa + c), v);
-      atomicAdd(args.K + (bp.oa + a) * n + kp.ob + d, f * v);
-    }
-#pragma unroll
-  for (int b = 0; b < C::NB; ++b)
-#pragma unroll
-    for (int d = 0; d < C::ND; ++d) {
-      double v = 0.0;
-#pragma unroll
-      for (int a = 0; a < C::NA; ++a)
-#pragma unroll
-        for (int c = 0; c < C::NC; ++c)
-          v = fma(acc[((a * C::NB + b) * C::NC + c) * C::ND + d], __ldg(D + (bp.oa + a) * n + kp.oa + c), v);
-      atomicAdd(args.K + (bp.ob + b) * n + kp.ob + d, f * v);
-    }
+  }  // task loop
 }
 
 // ---------------------------------------------------------------------------
@@ -359,93 +387,108 @@ __global__ void __launch_bounds__(128) store_kernel(StoreArgs args) {
 
 // ---------------------------------------------------------------------------
 // Two-electron gradient (eri_gradient_fused, scf/gradient.rs:1430-1640).
-template <int LA, int LB, int LC, int LD>
-__global__ void __launch_bounds__(128) grad_kernel(GradArgs args) {
+template <int LA, int LB, int LC, int LD, int G>
+__global__ void __launch_bounds__(128, (LA + LB + LC + LD <= 1) ? 4 : 1) grad_kernel(GradArgs args) {
   using C = Cls<LA, LB, LC, LD>;
-  // extended tables: a..d up to L+1, VRR to NBRA+1 / NKET+1
-  constexpr int EA = LA + 1, EB = LB + 1, EC = LC + 1, ED = LD + 1;
+  // tables extended by one on A, B, C; the D derivative follows from
+  // translational invariance, so D needs no extension
+  constexpr int EA = LA + 1, EB = LB + 1, EC = LC + 1, ED = LD;
   constexpr int ESZ = (EA + 1) * (EB + 1) * (EC + 1) * (ED + 1);
   auto eidx = [](int a, int b, int c, int d) { return ((a * (EB + 1) + b) * (EC + 1) + c) * (ED + 1) + d; };
   constexpr int NR = (LA + LB + LC + LD + 2) / 2 + 1;
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  constexpr int NG = 32 / G;
+  extern __shared__ double rtab[];
+  rys_stage_table<NR>(rtab);
+  // per-block gradient accumulator: many quartets hit the same few atoms, so
+  // global atomics would serialise; one flush per block at the end instead
+  double* gacc = rtab + rys_tab_doubles<NR>();
+  if (args.gsmem)
+    for (int i = threadIdx.x; i < 3 * args.natoms; i += blockDim.x) gacc[i] = 0.0;
+  __syncthreads();
+  double* gout = args.gsmem ? gacc : args.grad;
   const int lane = threadIdx.x & 31;
-  if (warp >= args.ntasks) return;
+  for (int warp = next_task(args.next_task, lane); warp < args.ntasks; warp = next_task(args.next_task, lane)) {
   const QuartetTask task = args.tasks[warp];
   const ShellPair bp = args.pairs[task.bra];
-  bool active = lane < task.nket;
-  ShellPair kp = bp;
-  int kpos = 0;
-  if (active) {
-    kpos = task.ket0 + lane;
-    kp = args.pairs[__ldg(args.ket_list + kpos)];
-    // the reference skips when the Schwarz bound of its bra pair (the larger
-    // composite index) is below threshold (gradient.rs:1457-1460)
-    const double qref = bp.comp >= kp.comp ? bp.Q : kp.Q;
-    if (qref < args.schwarz_thr) active = false;
-  }
-  double gA[3] = {0, 0, 0}, gB[3] = {0, 0, 0}, gC[3] = {0, 0, 0};
-  if (active) {
-    const int n = args.nbf;
-    const double* __restrict__ D = args.D;
-    const bool ij_same = bp.sa == bp.sb, kl_same = kp.sa == kp.sb;
-    const bool bk_same = task.diag && kpos == task.bra_pos;
-    const double xs = args.xscale;
-    double W[C::NCOMP];
+  const int grp = lane / G, sub = lane - grp * G;
+  const int n = args.nbf;
+  const double* __restrict__ D = args.D;
+  const double xs = args.xscale;
+  const bool ij_same = bp.sa == bp.sb;
+  const double AB[3] = {bp.A[0] - bp.B[0], bp.A[1] - bp.B[1], bp.A[2] - bp.B[2]};
+  double gA[3] = {0, 0, 0}, gB[3] = {0, 0, 0};
+  for (int kbase = 0; kbase < task.nket; kbase += NG) {
+    const int kk = kbase + grp;
+    bool active = kk < task.nket;
+    ShellPair kp = bp;
+    int kpos = 0;
+    if (active) {
+      kpos = task.ket0 + kk;
+      kp = args.pairs[__ldg(args.ket_list + kpos)];
+      // the reference skips when the Schwarz bound of its bra pair (the larger
+      // composite index) is below threshold (gradient.rs:1457-1460)
+      const double qref = bp.comp >= kp.comp ? bp.Q : kp.Q;
+      if (qref < args.schwarz_thr) active = false;
+    }
+    double gC[3] = {0, 0, 0}, gBq[3] = {0, 0, 0}, gAq[3] = {0, 0, 0};
+    if (active) {
+      const bool kl_same = kp.sa == kp.sb;
+      const bool bk_same = task.diag && kpos == task.bra_pos;
+      double W[C::NCOMP];
 #pragma unroll
-    for (int a = 0; a < C::NA; ++a)
+      for (int a = 0; a < C::NA; ++a)
 #pragma unroll
-      for (int b = 0; b < C::NB; ++b)
+        for (int b = 0; b < C::NB; ++b)
 #pragma unroll
-        for (int c = 0; c < C::NC; ++c)
+          for (int c = 0; c < C::NC; ++c)
 #pragma unroll
-          for (int d = 0; d < C::ND; ++d) {
-            const int i = bp.oa + a, j = bp.ob + b, k = kp.oa + c, l = kp.ob + d;
-            auto dd = [&](int x, int y) { return __ldg(D + x * n + y); };
-            auto w = [&](int p, int q2, int r, int s2) {
-              return 0.5 * dd(p, q2) * dd(r, s2) - xs * dd(p, r) * dd(q2, s2);
-            };
-            double t = w(i, j, k, l);
-            if (!ij_same) t += w(j, i, k, l);
-            if (!kl_same) t += w(i, j, l, k);
-            if (!ij_same && !kl_same) t += w(j, i, l, k);
-            if (!bk_same) {
-              t += w(k, l, i, j);
-              if (!kl_same) t += w(l, k, i, j);
-              if (!ij_same) t += w(k, l, j, i);
-              if (!ij_same && !kl_same) t += w(l, k, j, i);
+            for (int d = 0; d < C::ND; ++d) {
+              const int i = bp.oa + a, j = bp.ob + b, k = kp.oa + c, l = kp.ob + d;
+              const double dij = __ldg(D + i * n + j), dkl = __ldg(D + k * n + l);
+              const double dik = __ldg(D + i * n + k), djl = __ldg(D + j * n + l);
+              const double dil = __ldg(D + i * n + l), djk = __ldg(D + j * n + k);
+              // compute_symmetry_weight (gradient.rs:1570-1640) with D symmetric
+              double t = 0.5 * dij * dkl - xs * dik * djl;
+              if (!ij_same) t += 0.5 * dij * dkl - xs * djk * dil;
+              if (!kl_same) t += 0.5 * dij * dkl - xs * dil * djk;
+              if (!ij_same && !kl_same) t += 0.5 * dij * dkl - xs * djl * dik;
+              if (!bk_same) {
+                t += 0.5 * dkl * dij - xs * dik * djl;
+                if (!kl_same) t += 0.5 * dkl * dij - xs * dil * djk;
+                if (!ij_same) t += 0.5 * dkl * dij - xs * djk * dil;
+                if (!ij_same && !kl_same) t += 0.5 * dkl * dij - xs * djl * dik;
+              }
+              // D is angular-scaled: t = w_ref * (ang_a ang_b ang_c ang_d); the
+              // |w| < 1e-15 skip applies to the reference weight w_ref
+              const double angp = ang_factor(LA, a) * ang_factor(LB, b) * ang_factor(LC, c) * ang_factor(LD, d);
+              W[((a * C::NB + b) * C::NC + c) * C::ND + d] = (fabs(t / angp) < 1e-15) ? 0.0 : t;
             }
-            const double angp = ang_factor(LA, a) * ang_factor(LB, b) * ang_factor(LC, c) * ang_factor(LD, d);
-            // D here is angular-scaled, so t * angp is the reference weight
-            // divided by angp again; the |w| < 1e-15 skip applies to the
-            // reference weight: w_ref = t / angp^... -> t is w_ref/angp^1
-            W[((a * C::NB + b) * C::NC + c) * C::ND + d] = (fabs(t / angp) < 1e-15) ? 0.0 : t;
-          }
-    const double AB[3] = {bp.A[0] - bp.B[0], bp.A[1] - bp.B[1], bp.A[2] - bp.B[2]};
-    const double CD[3] = {kp.A[0] - kp.B[0], kp.A[1] - kp.B[1], kp.A[2] - kp.B[2]};
-    for (int i = 0; i < bp.np; ++i) {
-      const PrimPair b = load_pp(args.pp + bp.pstart + i);
-      for (int j = 0; j < kp.np; ++j) {
-        const PrimPair k = load_pp(args.pp + kp.pstart + j);
+      const double CD[3] = {kp.A[0] - kp.B[0], kp.A[1] - kp.B[1], kp.A[2] - kp.B[2]};
+      const int nitems = bp.np * kp.np;
+      for (int it = sub; it < nitems; it += G) {
+        const int pi = it / kp.np, pj = it - pi * kp.np;
+        const PrimPair b = load_pp(args.pp + bp.pstart + pi);
+        const PrimPair k = load_pp(args.pp + kp.pstart + pj);
         if (b.K * k.K < args.prim_thr) continue;
         const double p = b.p, q = k.p, s = p + q;
         const double PQ[3] = {b.P[0] - k.P[0], b.P[1] - k.P[1], b.P[2] - k.P[2]};
-        const double rho = p * q / s;
+        const double inv_s = 1.0 / s;
+        const double rho = p * q * inv_s;
         const double T = rho * (PQ[0] * PQ[0] + PQ[1] * PQ[1] + PQ[2] * PQ[2]);
-        const double pref = kTwoPi52 * b.cK * k.cK / (p * q * sqrt(s));
+        const double pref = kTwoPi52 * b.cK * k.cK * b.inv_p * k.inv_p * inv_s * sqrt(s);
         double rt[NR], wt[NR];
-        rys_rule<NR>(T, rt, wt);
+        rys_rule_tab<NR>(T, rtab, rt, wt);
         const double PA[3] = {b.P[0] - bp.A[0], b.P[1] - bp.A[1], b.P[2] - bp.A[2]};
         const double QC[3] = {k.P[0] - kp.A[0], k.P[1] - kp.A[1], k.P[2] - kp.A[2]};
-        const double a2 = 2.0 * b.aa, b2 = 2.0 * b.ab, c2 = 2.0 * k.aa;
+        const double a2 = 2.0 * b.aa, b2 = 2.0 * (b.p - b.aa), c2 = 2.0 * k.aa;
 #pragma unroll
         for (int r = 0; r < NR; ++r) {
           const double t2 = rt[r];
-          const double u = t2 < 1.0 - 1e-15 ? t2 / (1.0 - t2) : 1e15;
-          const double u2 = rho * u;
-          const double tmp4 = 0.5 / (u2 * s + p * q);
-          const double tmp5 = u2 * tmp4;
-          const double b00 = tmp5, b10 = tmp5 + tmp4 * q, b01 = tmp5 + tmp4 * p;
-          const double f2 = 2.0 * tmp5 * q, f3 = 2.0 * tmp5 * p;
+          // rys_coefficients.rs:94-180 with u2 (p+q) + pq = pq / (1 - t^2):
+          // tmp5 = t^2 / (2(p+q)), tmp4 q = (1 - t^2) / (2p), tmp4 p = (1 - t^2) / (2q)
+          const double b00 = 0.5 * t2 * inv_s, h = 0.5 - 0.5 * t2;
+          const double b10 = fma(h, b.inv_p, b00), b01 = fma(h, k.inv_p, b00);
+          const double f2 = t2 * q * inv_s, f3 = t2 * p * inv_s;
           double E[3][ESZ];
 #pragma unroll
           for (int ax = 0; ax < 3; ++ax)
@@ -461,18 +504,11 @@ __global__ void __launch_bounds__(128) grad_kernel(GradArgs args) {
 #pragma unroll
                 for (int d = 0; d < C::ND; ++d) {
                   const double w = W[((a * C::NB + bb) * C::NC + c) * C::ND + d];
-                  int pw[4][3];
-#pragma unroll
-                  for (int ax = 0; ax < 3; ++ax) {
-                    pw[0][ax] = cart_pow(LA, a, ax);
-                    pw[1][ax] = cart_pow(LB, bb, ax);
-                    pw[2][ax] = cart_pow(LC, c, ax);
-                    pw[3][ax] = cart_pow(LD, d, ax);
-                  }
                   double reg[3], dA[3], dB[3], dC[3];
 #pragma unroll
                   for (int ax = 0; ax < 3; ++ax) {
-                    const int ia = pw[0][ax], ib = pw[1][ax], ic = pw[2][ax], id = pw[3][ax];
+                    const int ia = cart_pow(LA, a, ax), ib = cart_pow(LB, bb, ax), ic = cart_pow(LC, c, ax),
+                              id = cart_pow(LD, d, ax);
                     reg[ax] = E[ax][eidx(ia, ib, ic, id)];
                     dA[ax] = a2 * E[ax][eidx(ia + 1, ib, ic, id)] -
                              (ia > 0 ? double(ia) * E[ax][eidx(ia > 0 ? ia - 1 : 0, ib, ic, id)] : 0.0);
@@ -482,79 +518,42 @@ __global__ void __launch_bounds__(128) grad_kernel(GradArgs args) {
                              (ic > 0 ? double(ic) * E[ax][eidx(ia, ib, ic > 0 ? ic - 1 : 0, id)] : 0.0);
                   }
                   const double wyz = w * reg[1] * reg[2], wxz = w * reg[0] * reg[2], wxy = w * reg[0] * reg[1];
-                  gA[0] = fma(wyz, dA[0], gA[0]); gA[1] = fma(wxz, dA[1], gA[1]); gA[2] = fma(wxy, dA[2], gA[2]);
-                  gB[0] = fma(wyz, dB[0], gB[0]); gB[1] = fma(wxz, dB[1], gB[1]); gB[2] = fma(wxy, dB[2], gB[2]);
+                  gAq[0] = fma(wyz, dA[0], gAq[0]); gAq[1] = fma(wxz, dA[1], gAq[1]); gAq[2] = fma(wxy, dA[2], gAq[2]);
+                  gBq[0] = fma(wyz, dB[0], gBq[0]); gBq[1] = fma(wxz, dB[1], gBq[1]); gBq[2] = fma(wxy, dB[2], gBq[2]);
                   gC[0] = fma(wyz, dC[0], gC[0]); gC[1] = fma(wxz, dC[1], gC[1]); gC[2] = fma(wxy, dC[2], gC[2]);
                 }
         }
       }
     }
+    // ket atoms differ per group: segmented reduction, lane 0 of the group adds
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+      const double c = group_sum<G>(gC[x]);
+      const double dsum = group_sum<G>(gAq[x] + gBq[x] + gC[x]);
+      if (active && sub == 0) {
+        atomicAdd(gout + 3 * kp.atom_a + x, c);
+        atomicAdd(gout + 3 * kp.atom_b + x, -dsum);  // translational invariance
+      }
+      gA[x] += gAq[x];
+      gB[x] += gBq[x];
+    }
   }
-  // bra atoms are shared by the warp: reduce, then one atomic per component
-  double* g = args.grad;
+  // bra atoms are shared by the whole warp: one reduction per task
 #pragma unroll
   for (int x = 0; x < 3; ++x) {
     const double sa = warp_sum(gA[x]);
     const double sb = warp_sum(gB[x]);
     if (lane == 0) {
-      atomicAdd(g + 3 * bp.atom_a + x, sa);
-      atomicAdd(g + 3 * bp.atom_b + x, sb);
-    }
-    if (active) {
-      // translational invariance: dD = -(dA + dB + dC)
-      atomicAdd(g + 3 * kp.atom_a + x, gC[x]);
-      atomicAdd(g + 3 * kp.atom_b + x, -(gA[x] + gB[x] + gC[x]));
+      atomicAdd(gout + 3 * bp.atom_a + x, sa);
+      atomicAdd(gout + 3 * bp.atom_b + x, sb);
     }
   }
-}
-
-// ---------------------------------------------------------------------------
-// Launchers for one bra class (LA, LB) against every ket class Y <= X.
-#define IQCP_KET_DISPATCH(X, Y, MACRO)                \
-  switch (Y) {                                        \
-    case 0: MACRO(0, 0); break;                       \
-    case 1: if (X >= 1) { MACRO(1, 0); } break;       \
-    case 2: if (X >= 2) { MACRO(1, 1); } break;       \
-    case 3: if (X >= 3) { MACRO(2, 0); } break;       \
-    case 4: if (X >= 4) { MACRO(2, 1); } break;       \
-    case 5: if (X >= 5) { MACRO(2, 2); } break;       \
-    default: return cudaErrorInvalidValue;            \
+  }  // task loop
+  if (args.gsmem) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < 3 * args.natoms; i += blockDim.x)
+      if (gacc[i] != 0.0) atomicAdd(args.grad + i, gacc[i]);
   }
-
-template <int LA, int LB>
-cudaError_t launch_jk_bra(int Y, const JKArgs& a, cudaStream_t st) {
-  constexpr int X = pair_class(LA, LB);
-  const int blocks = (a.ntasks + 3) / 4;
-#define LJK(lc, ld)                                                                    \
-  if constexpr (pair_class(lc, ld) <= X) {                                             \
-    if (a.K) jk_kernel<LA, LB, lc, ld, true><<<blocks, 128, 0, st>>>(a);               \
-    else jk_kernel<LA, LB, lc, ld, false><<<blocks, 128, 0, st>>>(a);                  \
-  }
-  IQCP_KET_DISPATCH(X, Y, LJK)
-#undef LJK
-  return cudaGetLastError();
-}
-
-template <int LA, int LB>
-cudaError_t launch_store_bra(int Y, const StoreArgs& a, cudaStream_t st) {
-  constexpr int X = pair_class(LA, LB);
-  const int blocks = (a.ntasks + 3) / 4;
-#define LST(lc, ld) \
-  if constexpr (pair_class(lc, ld) <= X) { store_kernel<LA, LB, lc, ld><<<blocks, 128, 0, st>>>(a); }
-  IQCP_KET_DISPATCH(X, Y, LST)
-#undef LST
-  return cudaGetLastError();
-}
-
-template <int LA, int LB>
-cudaError_t launch_grad_bra(int Y, const GradArgs& a, cudaStream_t st) {
-  constexpr int X = pair_class(LA, LB);
-  const int blocks = (a.ntasks + 3) / 4;
-#define LGR(lc, ld) \
-  if constexpr (pair_class(lc, ld) <= X) { grad_kernel<LA, LB, lc, ld><<<blocks, 128, 0, st>>>(a); }
-  IQCP_KET_DISPATCH(X, Y, LGR)
-#undef LGR
-  return cudaGetLastError();
 }
 
 }  // namespace iqcp

@@ -26,7 +26,7 @@
 typedef __float128 q;
 
 static const int kMaxN = 7;
-static const int kDeg = 13;          // Chebyshev degree per interval
+static const int kDeg = 11;          // Chebyshev degree per interval
 static const double kWidth = 1.0;    // interval width in T
 
 // F_k(T) = int_0^1 t^{2k} e^{-T t^2} dt, k = 0..m, by the series of F_m and
@@ -202,6 +202,9 @@ int main(int argc, char** argv) {
   fprintf(f, "// Generated by gen_rys_tables.cpp (binary128 Rys rules, Chebyshev fits). Do not edit.\n");
   fprintf(f, "#define RYS_TAB_MAXN %d\n#define RYS_TAB_DEG %d\n#define RYS_TAB_WIDTH %.1f\n", kMaxN, kDeg, kWidth);
   fprintf(f, "#ifndef RYS_TAB_QUAL\n#define RYS_TAB_QUAL static const\n#endif\n");
+  fprintf(f, "#define RYS_TAB_NINT {0");
+  for (int n = 1; n <= kMaxN; ++n) fprintf(f, ", %d", tasym[n]);
+  fprintf(f, "}\n");
   fprintf(f, "RYS_TAB_QUAL int kRysTasym[%d] = {0", kMaxN + 1);
   for (int n = 1; n <= kMaxN; ++n) fprintf(f, ", %d", tasym[n]);
   fprintf(f, "};\nRYS_TAB_QUAL int kRysOffset[%d] = {0", kMaxN + 2);

@@ -27,6 +27,7 @@ struct TaskRange {
   int X, Y;
   int first, count;         // into the task array
   long long quartets;       // screened shell quartets in the range
+  int mode[2];              // kernel variant for J/K [0] and gradient [1]
 };
 
 }  // namespace
@@ -50,6 +51,12 @@ struct iqcp_ctx {
   double* d_Kt = nullptr;
   double* d_io[4] = {nullptr, nullptr, nullptr, nullptr};  // staging for host-buffer calls
   double* d_grad = nullptr;
+  // mixed precision: per shell-pair max |D| and the FP32 quartet counter
+  double* d_dmax = nullptr;
+  unsigned long long* d_fp32 = nullptr;
+  int* d_counters = nullptr;      // one work counter per class range and kind
+  int* cur_counter = nullptr;
+  bool mixed_call = false;
   // basis copy for the one-electron kernel
   int* d_bint = nullptr;          // l | nprim | pstart | off | z
   double* d_bdbl = nullptr;       // center | exps | coefs | atom_xyz
@@ -116,6 +123,11 @@ int basis_id(const char* name) {
 }
 
 // Build class lists and quartet tasks from Schwarz bounds held in ctx->pairs.
+// Each class list is split into buckets of equal primitive-pair count (so the
+// 32 kets of a warp share one primitive-loop length), each bucket sorted by Q
+// descending so that the Schwarz test Q_bra * Q_ket >= thr keeps a prefix of
+// it.  Unique quartets of a class with itself keep ket position <= bra position
+// in the concatenated list.
 void build_tasks(iqcp_ctx* ctx, std::vector<int>& ket_list, std::vector<QuartetTask>& tasks) {
   const double thr = ctx->opt.schwarz_threshold;
   ctx->classes.assign(kNumPairClasses, ClassList());
@@ -125,10 +137,21 @@ void build_tasks(iqcp_ctx* ctx, std::vector<int>& ket_list, std::vector<QuartetT
     ctx->classes[cls].pairs.push_back(i);
   }
   ctx->list_offset.assign(kNumPairClasses + 1, 0);
+  std::vector<std::vector<std::pair<int, int>>> buckets(kNumPairClasses);  // [start, end) per class
   ket_list.clear();
   for (int c = 0; c < kNumPairClasses; ++c) {
     auto& v = ctx->classes[c].pairs;
-    std::stable_sort(v.begin(), v.end(), [&](int a, int b) { return ctx->pairs[a].Q > ctx->pairs[b].Q; });
+    std::stable_sort(v.begin(), v.end(), [&](int a, int b) {
+      const ShellPair &pa = ctx->pairs[a], &pb = ctx->pairs[b];
+      if (pa.np != pb.np) return pa.np > pb.np;
+      return pa.Q > pb.Q;
+    });
+    for (size_t s = 0; s < v.size();) {
+      size_t e = s;
+      while (e < v.size() && ctx->pairs[v[e]].np == ctx->pairs[v[s]].np) ++e;
+      buckets[c].push_back({(int)s, (int)e});
+      s = e;
+    }
     ctx->list_offset[c] = (int)ket_list.size();
     ket_list.insert(ket_list.end(), v.begin(), v.end());
   }
@@ -140,28 +163,31 @@ void build_tasks(iqcp_ctx* ctx, std::vector<int>& ket_list, std::vector<QuartetT
     for (int Y = 0; Y <= X; ++Y) {
       const auto& LX = ctx->classes[X].pairs;
       const auto& LY = ctx->classes[Y].pairs;
-      TaskRange r{X, Y, (int)tasks.size(), 0, 0};
+      TaskRange r{X, Y, (int)tasks.size(), 0, 0, {default_mode(X, Y, 0), default_mode(X, Y, 1)}};
       for (int b = 0; b < (int)LX.size(); ++b) {
         const double qb = ctx->pairs[LX[b]].Q;
-        // ket prefix with qb*qk >= thr (lists sorted by Q descending)
-        int lo = 0, hi = (int)LY.size();
-        while (lo < hi) {
-          const int mid = (lo + hi) / 2;
-          if (qb * ctx->pairs[LY[mid]].Q < thr) hi = mid; else lo = mid + 1;
-        }
-        int nk = lo;
-        if (X == Y) nk = std::min(nk, b + 1);
-        ctx->n_quartets += nk;
-        r.quartets += nk;
-        for (int k0 = 0; k0 < nk; k0 += 32) {
-          QuartetTask t;
-          t.bra = LX[b];
-          t.ket0 = ctx->list_offset[Y] + k0;
-          t.nket = std::min(32, nk - k0);
-          t.diag = (X == Y) ? 1 : 0;
-          t.bra_pos = ctx->list_offset[X] + b;
-          t.flags = 0;
-          tasks.push_back(t);
+        for (const auto& bk : buckets[Y]) {
+          if (X == Y && bk.first > b) break;
+          const int hi_pos = (X == Y) ? std::min(bk.second, b + 1) : bk.second;
+          // prefix of the bucket with qb * qk >= thr
+          int lo = bk.first, hi = hi_pos;
+          while (lo < hi) {
+            const int mid = (lo + hi) / 2;
+            if (qb * ctx->pairs[LY[mid]].Q < thr) hi = mid; else lo = mid + 1;
+          }
+          const int nk = lo - bk.first;
+          ctx->n_quartets += nk;
+          r.quartets += nk;
+          for (int k0 = 0; k0 < nk; k0 += 32) {
+            QuartetTask t;
+            t.bra = LX[b];
+            t.ket0 = ctx->list_offset[Y] + bk.first + k0;
+            t.nket = std::min(32, nk - k0);
+            t.diag = (X == Y) ? 1 : 0;
+            t.bra_pos = ctx->list_offset[X] + b;
+            t.flags = 0;
+            tasks.push_back(t);
+          }
         }
       }
       r.count = (int)tasks.size() - r.first;
@@ -187,17 +213,21 @@ int ensure_profile_events(iqcp_ctx* ctx) {
 // Launch one quartet kernel per non-empty class range; kind 0 = J/K, 1 = gradient.
 template <typename F>
 int run_ranges(iqcp_ctx* ctx, int kind, F&& launch) {
+  // launch(r) reads ctx->cur_counter for the range's work counter
   if (ctx->profile) {
     int rc = ensure_profile_events(ctx);
     if (rc) return rc;
   }
   ctx->launch_log.clear();
+  CK(cudaMemsetAsync(ctx->d_counters + kind * ctx->ranges.size(), 0, sizeof(int) * ctx->ranges.size(),
+                     ctx->stream));
   CK(cudaEventRecord(ctx->ev0, ctx->stream));
   int launches = 0;
   for (size_t i = 0; i < ctx->ranges.size(); ++i) {
     const TaskRange& r = ctx->ranges[i];
     if (r.count == 0) continue;
     if (ctx->profile) CK(cudaEventRecord(ctx->pev[2 * i], ctx->stream));
+    ctx->cur_counter = ctx->d_counters + kind * ctx->ranges.size() + i;
     CK(launch(r));
     if (ctx->profile) CK(cudaEventRecord(ctx->pev[2 * i + 1], ctx->stream));
     ++launches;
@@ -215,6 +245,13 @@ int run_jk_device(iqcp_ctx* ctx, const double* dD, bool want_k) {
   const size_t bytes = sizeof(double) * (size_t)n * n;
   ctx->launches_total = 1;
   CK(launch_scale_density(dD, ctx->d_ang, n, ctx->d_Ds, ctx->stream));
+  ctx->mixed_call = ctx->opt.precision == IQCP_MIXED;
+  if (ctx->mixed_call) {
+    CK(launch_shell_dmax(dD, ctx->d_bint + 3 * ctx->n_shells, ctx->d_bint, ctx->n_shells, n, ctx->d_dmax,
+                         ctx->stream));
+    CK(cudaMemsetAsync(ctx->d_fp32, 0, sizeof(unsigned long long), ctx->stream));
+    ctx->launches_total += 1;
+  }
   CK(cudaMemsetAsync(ctx->d_Jt, 0, bytes, ctx->stream));
   if (want_k) CK(cudaMemsetAsync(ctx->d_Kt, 0, bytes, ctx->stream));
   return run_ranges(ctx, 0, [&](const TaskRange& r) {
@@ -229,6 +266,12 @@ int run_jk_device(iqcp_ctx* ctx, const double* dD, bool want_k) {
     a.J = ctx->d_Jt;
     a.K = want_k ? ctx->d_Kt : nullptr;
     a.prim_thr = ctx->opt.prim_threshold;
+    a.mode = r.mode[0];
+    a.dmax_shell = ctx->mixed_call ? ctx->d_dmax : nullptr;
+    a.n_shells = ctx->n_shells;
+    a.mixed_cutoff = ctx->opt.mixed_cutoff;
+    a.fp32_count = ctx->mixed_call ? ctx->d_fp32 : nullptr;
+    a.next_task = ctx->cur_counter;
     return launch_jk(r.X, r.Y, a, ctx->stream);
   });
 }
@@ -238,6 +281,13 @@ int finish_stats(iqcp_ctx* ctx) {
   CK(cudaEventSynchronize(ctx->ev1));
   CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
   ctx->stats[2] = ms * 1e3;
+  ctx->stats[3] = 0.0;
+  if (ctx->mixed_call) {
+    unsigned long long c = 0;
+    CK(cudaMemcpyAsync(&c, ctx->d_fp32, sizeof(c), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->stats[3] = (double)c;
+  }
   if (ctx->profile) {
     size_t k = 0;
     for (size_t i = 0; i < ctx->ranges.size(); ++i) {
@@ -392,7 +442,7 @@ int iqcp_create(const iqcp_basis_desc* b, const iqcp_options* opts, iqcp_ctx** o
           q.cK = K * b->coefs[pstart[sa] + i] * rad_norm(ea, b->l[sa]) * b->coefs[pstart[sb] + j] *
                  rad_norm(eb, b->l[sb]);
           q.aa = ea;
-          q.ab = eb;
+          q.inv_p = 1.0 / q.p;
           pps.push_back(q);
         }
       sp.np = (int)pps.size() - sp.pstart;
@@ -446,6 +496,9 @@ int iqcp_create(const iqcp_basis_desc* b, const iqcp_options* opts, iqcp_ctx** o
   CK(cudaMalloc(&ctx->d_Kt, sizeof(double) * nn));
   for (int i = 0; i < 4; ++i) CK(cudaMalloc(&ctx->d_io[i], sizeof(double) * nn));
   CK(cudaMalloc(&ctx->d_grad, sizeof(double) * 3 * ctx->n_atoms));
+  CK(cudaMalloc(&ctx->d_dmax, sizeof(double) * (size_t)ctx->n_shells * ctx->n_shells));
+  CK(cudaMalloc(&ctx->d_counters, sizeof(int) * 2 * (ctx->ranges.size() + 1)));
+  CK(cudaMalloc(&ctx->d_fp32, sizeof(unsigned long long)));
   return IQCP_OK;
 }
 
@@ -465,6 +518,9 @@ void iqcp_destroy(iqcp_ctx* ctx) {
   cudaFree(ctx->d_grad);
   cudaFree(ctx->d_bint);
   cudaFree(ctx->d_bdbl);
+  cudaFree(ctx->d_dmax);
+  cudaFree(ctx->d_counters);
+  cudaFree(ctx->d_fp32);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
@@ -564,6 +620,7 @@ int iqcp_jk_device_noalloc(iqcp_ctx* ctx, const double* dD, double* dJ, double* 
   const bool want_k = dK != nullptr;
   const bool prof = ctx->profile;
   ctx->profile = false;  // per-launch timing would create events
+  ctx->mixed_call = false;
   ctx->launches_total = 1;
   CK(launch_scale_density(dD, ctx->d_ang, n, Ds, ctx->stream));
   CK(cudaMemsetAsync(Jt, 0, sizeof(double) * nn, ctx->stream));
@@ -580,6 +637,12 @@ int iqcp_jk_device_noalloc(iqcp_ctx* ctx, const double* dD, double* dJ, double* 
     a.J = Jt;
     a.K = want_k ? Kt : nullptr;
     a.prim_thr = ctx->opt.prim_threshold;
+    a.mode = r.mode[0];
+    a.dmax_shell = nullptr;  // FP64 only
+    a.n_shells = ctx->n_shells;
+    a.mixed_cutoff = 0.0;
+    a.fp32_count = nullptr;
+    a.next_task = ctx->cur_counter;
     return launch_jk(r.X, r.Y, a, ctx->stream);
   });
   ctx->profile = prof;
@@ -631,6 +694,7 @@ int iqcp_eri_grad_device(iqcp_ctx* ctx, const double* dD, double hf_frac, double
   if (rc) return rc;
   const int n = ctx->nbf;
   ctx->launches_total = 1;
+  ctx->mixed_call = false;
   CK(launch_scale_density(dD, ctx->d_ang, n, ctx->d_Ds, ctx->stream));
   rc = run_ranges(ctx, 1, [&](const TaskRange& r) {
     GradArgs a;
@@ -645,6 +709,10 @@ int iqcp_eri_grad_device(iqcp_ctx* ctx, const double* dD, double hf_frac, double
     a.grad = dgrad;
     a.prim_thr = ctx->opt.prim_threshold;
     a.schwarz_thr = ctx->opt.schwarz_threshold;
+    a.natoms = ctx->n_atoms;
+    a.gsmem = ctx->n_atoms <= 2048 ? 1 : 0;
+    a.mode = r.mode[1];
+    a.next_task = ctx->cur_counter;
     return launch_grad(r.X, r.Y, a, ctx->stream);
   });
   if (rc) return rc;
@@ -733,6 +801,13 @@ int iqcp_schwarz(iqcp_ctx* ctx, double* Q) {
   return IQCP_OK;
 }
 
+int iqcp_set_precision(iqcp_ctx* ctx, int precision, double mixed_cutoff) {
+  if (!ctx || (precision != IQCP_FP64 && precision != IQCP_MIXED) || !(mixed_cutoff >= 0.0)) return IQCP_ERR_ARG;
+  ctx->opt.precision = precision;
+  ctx->opt.mixed_cutoff = mixed_cutoff;
+  return IQCP_OK;
+}
+
 int iqcp_set_profiling(iqcp_ctx* ctx, int on) {
   if (!ctx) return IQCP_ERR_ARG;
   ctx->profile = on != 0;
@@ -754,6 +829,90 @@ int iqcp_launch_profile(const iqcp_ctx* ctx, int max, int* kind, int* X, int* Y,
 }
 
 int iqcp_kernel_launches(const iqcp_ctx* ctx) { return ctx ? ctx->launches_total : 0; }
+
+// Autotuner: time every class range with every kernel variant on this
+// density (best of `reps` runs each) and keep the fastest variant per class
+// and per kind (J/K, gradient).  Results are the same up to rounding whichever
+// variant runs; only the speed differs.
+int iqcp_autotune(iqcp_ctx* ctx, const double* dD, int reps) {
+  if (!ctx || !dD) return IQCP_ERR_ARG;
+  int rc = ensure_device(ctx);
+  if (rc) return rc;
+  if (reps < 1) reps = 1;
+  const int n = ctx->nbf;
+  const size_t bytes = sizeof(double) * (size_t)n * n;
+  CK(launch_scale_density(dD, ctx->d_ang, n, ctx->d_Ds, ctx->stream));
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  for (int kind = 0; kind < 2; ++kind) {
+    for (TaskRange& r : ctx->ranges) {
+      if (r.count == 0) continue;
+      float best = 1e30f;
+      int best_mode = r.mode[kind];
+      for (int mode = 0; mode < kNumModes; ++mode) {
+        float tmin = 1e30f;
+        for (int rep = 0; rep < reps + 1; ++rep) {  // first run warms caches and sets attributes
+          CK(cudaMemsetAsync(ctx->d_Jt, 0, bytes, ctx->stream));
+          CK(cudaMemsetAsync(ctx->d_Kt, 0, bytes, ctx->stream));
+          CK(cudaMemsetAsync(ctx->d_grad, 0, sizeof(double) * 3 * ctx->n_atoms, ctx->stream));
+          CK(cudaMemsetAsync(ctx->d_counters, 0, sizeof(int), ctx->stream));
+          CK(cudaEventRecord(e0, ctx->stream));
+          if (kind == 0) {
+            JKArgs a;
+            a.pairs = ctx->d_pairs; a.pp = ctx->d_pp; a.ket_list = ctx->d_ket_list;
+            a.tasks = ctx->d_tasks + r.first; a.ntasks = r.count; a.D = ctx->d_Ds; a.nbf = n;
+            a.J = ctx->d_Jt; a.K = ctx->d_Kt; a.prim_thr = ctx->opt.prim_threshold; a.mode = mode;
+            a.dmax_shell = nullptr; a.n_shells = ctx->n_shells; a.mixed_cutoff = 0.0; a.fp32_count = nullptr;
+            a.next_task = ctx->d_counters;
+            CK(launch_jk(r.X, r.Y, a, ctx->stream));
+          } else {
+            GradArgs a;
+            a.pairs = ctx->d_pairs; a.pp = ctx->d_pp; a.ket_list = ctx->d_ket_list;
+            a.tasks = ctx->d_tasks + r.first; a.ntasks = r.count; a.D = ctx->d_Ds; a.nbf = n;
+            a.xscale = 0.25; a.grad = ctx->d_grad; a.prim_thr = ctx->opt.prim_threshold;
+            a.schwarz_thr = ctx->opt.schwarz_threshold;
+    a.natoms = ctx->n_atoms;
+    a.gsmem = ctx->n_atoms <= 2048 ? 1 : 0; a.mode = mode;
+            a.next_task = ctx->d_counters;
+            CK(launch_grad(r.X, r.Y, a, ctx->stream));
+          }
+          CK(cudaEventRecord(e1, ctx->stream));
+          CK(cudaEventSynchronize(e1));
+          float ms = 0.f;
+          CK(cudaEventElapsedTime(&ms, e0, e1));
+          if (rep > 0) tmin = std::min(tmin, ms);
+        }
+        if (tmin < best) {
+          best = tmin;
+          best_mode = mode;
+        }
+      }
+      r.mode[kind] = best_mode;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return IQCP_OK;
+}
+
+// Current kernel variant per (kind, bra class, ket class): modes[2*6*6], -1 when no work.
+int iqcp_kernel_modes(const iqcp_ctx* ctx, int* modes) {
+  if (!ctx || !modes) return IQCP_ERR_ARG;
+  for (int i = 0; i < 2 * kNumPairClasses * kNumPairClasses; ++i) modes[i] = -1;
+  for (const TaskRange& r : ctx->ranges)
+    if (r.count > 0)
+      for (int kind = 0; kind < 2; ++kind)
+        modes[(kind * kNumPairClasses + r.X) * kNumPairClasses + r.Y] = r.mode[kind];
+  return IQCP_OK;
+}
+
+int iqcp_set_kernel_mode(iqcp_ctx* ctx, int kind, int X, int Y, int mode) {
+  if (!ctx || kind < 0 || kind > 1 || mode < 0 || mode >= kNumModes) return IQCP_ERR_ARG;
+  for (TaskRange& r : ctx->ranges)
+    if ((X < 0 || r.X == X) && (Y < 0 || r.Y == Y)) r.mode[kind] = mode;
+  return IQCP_OK;
+}
 
 static int count_prim_quartets(iqcp_ctx* ctx) {
   if (!ctx->prim_quartets.empty()) return IQCP_OK;

@@ -5,7 +5,7 @@
 // computes them per call from moments with Schmidt orthogonalisation and a
 // companion-matrix QR (rys/mod.rs:468-790).  On the device a per-call
 // eigen-solve diverges across lanes, so the rule is read from tables instead:
-// degree-13 Chebyshev series on unit intervals of T up to Tasym(n), and the
+// degree-11 Chebyshev series on unit intervals of T up to Tasym(n), and the
 // large-T Hermite limit (roots y_i/T, weights W_i/sqrt(T)) beyond it.  The
 // tables (rys_tables.inc, made by gen_rys_tables.cpp in binary128) are exact
 // to ~3e-16 relative, i.e. closer to the true rule than the reference's own
@@ -22,6 +22,61 @@
 #undef RYS_TAB_QUAL
 
 namespace iqcp {
+
+// unit intervals below Tasym(n)
+__host__ __device__ constexpr int rys_nint(int n) {
+  constexpr int t[RYS_TAB_MAXN + 1] = RYS_TAB_NINT;
+  return t[n];
+}
+// doubles in the order-N table: [interval][root 0..N-1, weight 0..N-1][coefficient]
+template <int N>
+__host__ __device__ constexpr int rys_tab_doubles() { return rys_nint(N) * 2 * N * (RYS_TAB_DEG + 1); }
+
+// Copy the order-N table into shared memory (all threads of the block).  Each
+// lane reads the interval of its own T, so table reads are scattered: from
+// shared memory they cost a few bank wavefronts, from L1 one cache line per lane.
+template <int N>
+__device__ __forceinline__ void rys_stage_table(double* __restrict__ s) {
+  const double* g = kRysCheb + kRysOffset[N];
+  for (int i = threadIdx.x; i < rys_tab_doubles<N>(); i += blockDim.x) s[i] = __ldg(g + i);
+}
+
+__device__ __forceinline__ double cheb_clenshaw_s(const double* c, double x2) {
+  double b1 = 0.0, b2 = 0.0;
+#pragma unroll
+  for (int j = RYS_TAB_DEG; j >= 1; --j) {
+    const double t = fma(x2, b1, c[j] - b2);
+    b2 = b1;
+    b1 = t;
+  }
+  return fma(0.5 * x2, b1, c[0] - b2);
+}
+
+// rys_rule with the order-N table staged in shared memory at `s`
+template <int N>
+__device__ __forceinline__ void rys_rule_tab(double T, const double* s, double* __restrict__ r,
+                                             double* __restrict__ w) {
+  constexpr int NI = rys_nint(N);
+  if (T >= double(NI)) {
+    const double it = 1.0 / T;
+    const double is = 1.0 / sqrt(T);
+    const int base = (N * (N - 1)) / 2;
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+      r[i] = __ldg(kRysAsymRoot + base + i) * it;
+      w[i] = __ldg(kRysAsymWeight + base + i) * is;
+    }
+    return;
+  }
+  const int k = int(T);
+  const double x2 = 2.0 * (2.0 * (T - double(k)) - 1.0);
+  const double* c = s + k * (2 * N * (RYS_TAB_DEG + 1));
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    r[i] = cheb_clenshaw_s(c + i * (RYS_TAB_DEG + 1), x2);
+    w[i] = cheb_clenshaw_s(c + (N + i) * (RYS_TAB_DEG + 1), x2);
+  }
+}
 
 __device__ __forceinline__ double cheb_clenshaw(const double* __restrict__ c, double x2) {
   // x2 = 2x; sum_j c_j T_j(x)
