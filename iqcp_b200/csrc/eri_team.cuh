@@ -31,7 +31,7 @@ __device__ __forceinline__ void rys_rule_one(double T, int r, const double* s, d
   }
   const int k = int(T);
   const double x2 = 2.0 * (2.0 * (T - double(k)) - 1.0);
-  const double* c = s + k * (2 * N * (RYS_TAB_DEG + 1));
+  const double* c = s + k * rys_tab_stride<N>();
   *t2 = cheb_clenshaw_s(c + r * (RYS_TAB_DEG + 1), x2);
   *w = cheb_clenshaw_s(c + (N + r) * (RYS_TAB_DEG + 1), x2);
 }

@@ -124,12 +124,20 @@ __device__ __forceinline__ void quartet_fp64(const ShellPair& bp, const ShellPai
   for (int i = 0; i < C::NCOMP; ++i) acc[i] = 0.0;
   const double AB[3] = {bp.A[0] - bp.B[0], bp.A[1] - bp.B[1], bp.A[2] - bp.B[2]};
   const double CD[3] = {kp.A[0] - kp.B[0], kp.A[1] - kp.B[1], kp.A[2] - kp.B[2]};
+  // ket-major order: the bra primitive is the same on every lane of the warp
+  // (one broadcast line per load); each lane's own ket primitive, scattered
+  // across lanes, is loaded once per j
   const int nitems = bp.np * kp.np;
+  int jl = -1;
+  PrimPair k;
   for (int it = first; it < nitems; it += stride) {
-    const int i = it / kp.np, j = it - i * kp.np;
+    const int j = it / bp.np, i = it - j * bp.np;
+    if (j != jl) {
+      k = load_pp(pp + kp.pstart + j);
+      jl = j;
+    }
     const PrimPair b = load_pp(pp + bp.pstart + i);
     {
-      const PrimPair k = load_pp(pp + kp.pstart + j);
       if (b.K * k.K < thr) continue;
       const double p = b.p, q = k.p, s = p + q;
       const double PQ[3] = {b.P[0] - k.P[0], b.P[1] - k.P[1], b.P[2] - k.P[2]};
@@ -465,10 +473,16 @@ __global__ void __launch_bounds__(128, (LA + LB + LC + LD <= 1) ? 4 : 1) grad_ke
             }
       const double CD[3] = {kp.A[0] - kp.B[0], kp.A[1] - kp.B[1], kp.A[2] - kp.B[2]};
       const int nitems = bp.np * kp.np;
+      int jl = -1;
+      PrimPair k;
       for (int it = sub; it < nitems; it += G) {
-        const int pi = it / kp.np, pj = it - pi * kp.np;
+        // ket-major order (see quartet_fp64)
+        const int pj = it / bp.np, pi = it - pj * bp.np;
+        if (pj != jl) {
+          k = load_pp(args.pp + kp.pstart + pj);
+          jl = pj;
+        }
         const PrimPair b = load_pp(args.pp + bp.pstart + pi);
-        const PrimPair k = load_pp(args.pp + kp.pstart + pj);
         if (b.K * k.K < args.prim_thr) continue;
         const double p = b.p, q = k.p, s = p + q;
         const double PQ[3] = {b.P[0] - k.P[0], b.P[1] - k.P[1], b.P[2] - k.P[2]};

@@ -28,17 +28,25 @@ __host__ __device__ constexpr int rys_nint(int n) {
   constexpr int t[RYS_TAB_MAXN + 1] = RYS_TAB_NINT;
   return t[n];
 }
-// doubles in the order-N table: [interval][root 0..N-1, weight 0..N-1][coefficient]
+// Shared-memory copy of the order-N table: [interval][root 0..N-1, weight
+// 0..N-1][coefficient], interval stride padded to an odd number of doubles so
+// that lanes reading different intervals fall on different bank pairs.
 template <int N>
-__host__ __device__ constexpr int rys_tab_doubles() { return rys_nint(N) * 2 * N * (RYS_TAB_DEG + 1); }
+__host__ __device__ constexpr int rys_tab_stride() { return 2 * N * (RYS_TAB_DEG + 1) + 1; }
+template <int N>
+__host__ __device__ constexpr int rys_tab_doubles() { return rys_nint(N) * rys_tab_stride<N>(); }
 
 // Copy the order-N table into shared memory (all threads of the block).  Each
 // lane reads the interval of its own T, so table reads are scattered: from
 // shared memory they cost a few bank wavefronts, from L1 one cache line per lane.
 template <int N>
 __device__ __forceinline__ void rys_stage_table(double* __restrict__ s) {
+  constexpr int W = 2 * N * (RYS_TAB_DEG + 1);
   const double* g = kRysCheb + kRysOffset[N];
-  for (int i = threadIdx.x; i < rys_tab_doubles<N>(); i += blockDim.x) s[i] = __ldg(g + i);
+  for (int i = threadIdx.x; i < rys_nint(N) * W; i += blockDim.x) {
+    const int k = i / W;
+    s[k * rys_tab_stride<N>() + (i - k * W)] = __ldg(g + i);
+  }
 }
 
 __device__ __forceinline__ double cheb_clenshaw_s(const double* c, double x2) {
@@ -70,7 +78,7 @@ __device__ __forceinline__ void rys_rule_tab(double T, const double* s, double* 
   }
   const int k = int(T);
   const double x2 = 2.0 * (2.0 * (T - double(k)) - 1.0);
-  const double* c = s + k * (2 * N * (RYS_TAB_DEG + 1));
+  const double* c = s + k * rys_tab_stride<N>();
 #pragma unroll
   for (int i = 0; i < N; ++i) {
     r[i] = cheb_clenshaw_s(c + i * (RYS_TAB_DEG + 1), x2);
