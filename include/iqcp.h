@@ -90,6 +90,21 @@ int iqcp_basis_build(const char* basis_name, int n_atoms, const int* z, const do
  */
 int iqcp_create(const iqcp_basis_desc* basis, const iqcp_options* opts, iqcp_ctx** out);
 void iqcp_destroy(iqcp_ctx* ctx);
+
+/*
+ * One context for many molecules (or geometries) of uneven size: every
+ * J/K, Fock, gradient and one-electron call then covers all of them with one
+ * launch per angular-momentum class.  Matrices are packed: molecule m owns the
+ * nbf[m] x nbf[m] row-major block at offset mat_offset[m]; gradient rows of
+ * molecule m are atoms [atom_offset[m], atom_offset[m+1]).  The quartet lists
+ * never pair shells of different molecules.  iqcp_batch_layout fills
+ * mat_offset[n_mol+1], nbf[n_mol], atom_offset[n_mol+1] (any may be NULL) and
+ * returns n_mol.  No counterpart in the reference, which loops over geometries
+ * (optimizer/mod.rs:274-320).  iqcp_eri_compressed, iqcp_jk_device_noalloc and
+ * the mixed form are single-geometry only.
+ */
+int iqcp_create_batch(int n_mol, const iqcp_basis_desc* bases, const iqcp_options* opts, iqcp_ctx** out);
+int iqcp_batch_layout(const iqcp_ctx* ctx, long long* mat_offset, int* nbf, int* atom_offset);
 const char* iqcp_last_error(const iqcp_ctx* ctx);
 int iqcp_nbf(const iqcp_ctx* ctx);
 

@@ -99,6 +99,9 @@ EXPORTS = {
     "iqcp_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]),
     "iqcp_kernel_modes": (ctypes.c_int, [ctypes.c_void_p, _c_int_p]),
     "iqcp_set_kernel_mode": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "iqcp_create_batch": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_BasisDesc), ctypes.POINTER(_Options),
+                                         ctypes.POINTER(ctypes.c_void_p)]),
+    "iqcp_batch_layout": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong), _c_int_p, _c_int_p]),
 }
 
 PAIR_CLASSES = ["ss", "ps", "pp", "ds", "dp", "dd"]
@@ -359,6 +362,97 @@ class FockEngine:
 
     def set_stream(self, stream_handle):
         self._check(self._lib.iqcp_set_stream(self._h, ctypes.c_void_p(stream_handle)))
+
+
+class BatchFockEngine(FockEngine):
+    """One context over many molecules or geometries (iqcp_create_batch).
+
+    Each call covers every molecule with one launch per angular-momentum
+    class.  Matrices travel packed: molecule m is the nbf[m] x nbf[m] block at
+    offset mat_offset[m] of one flat array; pack()/unpack() convert lists of
+    per-molecule matrices.  Gradients come back as a list of [n_atoms_m, 3]
+    arrays.
+    """
+
+    def __init__(self, bases, precision=FP64, schwarz_threshold=1e-12, prim_threshold=1e-15,
+                 mixed_cutoff=1e-9, device=0):
+        lib = load_library()
+        self._lib = lib
+        self.bases = list(bases)
+        self.basis = None
+        opts = _Options()
+        lib.iqcp_default_options(ctypes.byref(opts))
+        opts.schwarz_threshold = schwarz_threshold
+        opts.prim_threshold = prim_threshold
+        opts.precision = precision
+        opts.mixed_cutoff = mixed_cutoff
+        opts.device = device
+        n = len(self.bases)
+        self._descs = (_BasisDesc * n)(*[b._desc() for b in self.bases])
+        h = ctypes.c_void_p()
+        rc = lib.iqcp_create_batch(n, self._descs, ctypes.byref(opts), ctypes.byref(h))
+        self._h = h
+        if rc:
+            msg = lib.iqcp_last_error(h).decode() if h.value else ""
+            self.close()
+            raise IqcpError(rc, msg)
+        self.n_mol = n
+        self.mat_offset = np.zeros(n + 1, np.int64)
+        self.nbfs = np.zeros(n, np.int32)
+        self.atom_offset = np.zeros(n + 1, np.int32)
+        lib.iqcp_batch_layout(h, self.mat_offset.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong)),
+                              _ip(self.nbfs), _ip(self.atom_offset))
+        self.nbf = lib.iqcp_nbf(h)
+        self.packed_size = int(self.mat_offset[-1])
+        self.n_atoms = int(self.atom_offset[-1])
+
+    def pack(self, mats):
+        out = np.empty(self.packed_size)
+        for m, a in enumerate(mats):
+            n = int(self.nbfs[m])
+            a = np.asarray(a, dtype=np.float64)
+            if a.shape != (n, n):
+                raise ValueError("molecule %d: expected a %dx%d matrix" % (m, n, n))
+            out[self.mat_offset[m]:self.mat_offset[m + 1]] = a.ravel()
+        return out
+
+    def unpack(self, flat):
+        return [flat[self.mat_offset[m]:self.mat_offset[m + 1]].reshape(self.nbfs[m], self.nbfs[m]).copy()
+                for m in range(self.n_mol)]
+
+    def split_atoms(self, g):
+        g = np.asarray(g).reshape(-1, 3)
+        return [g[self.atom_offset[m]:self.atom_offset[m + 1]].copy() for m in range(self.n_mol)]
+
+    def build_jk(self, Ds, with_k=True):
+        D = self.pack(Ds)
+        J = np.empty_like(D)
+        K = np.empty_like(D) if with_k else None
+        self._check(self._lib.iqcp_jk(self._h, _dp(D), _dp(J), _dp(K) if with_k else None))
+        return (self.unpack(J), self.unpack(K)) if with_k else self.unpack(J)
+
+    def build_fock(self, Hs, Ds, k_scale=1.0):
+        H, D = self.pack(Hs), self.pack(Ds)
+        F = np.empty_like(D)
+        self._check(self._lib.iqcp_fock(self._h, _dp(H), _dp(D), float(k_scale), _dp(F)))
+        return self.unpack(F)
+
+    def eri_gradient(self, Ds, hf_frac=1.0):
+        D = self.pack(Ds)
+        g = np.zeros((self.n_atoms, 3))
+        self._check(self._lib.iqcp_eri_grad(self._h, _dp(D), float(hf_frac), _dp(g)))
+        return self.split_atoms(g)
+
+    def one_electron(self):
+        S, T, V = (np.empty(self.packed_size) for _ in range(3))
+        self._check(self._lib.iqcp_one_electron(self._h, _dp(S), _dp(T), _dp(V)))
+        return self.unpack(S), self.unpack(T), self.unpack(V)
+
+    def eri_compressed(self):
+        raise IqcpError(-1, "stored ERIs are single-geometry only")
+
+    def jk_device_noalloc(self, d_D, d_J, d_K=None):
+        raise IqcpError(-1, "the fixed-scratch form is single-geometry only")
 
 
 def boys_eval_all(m_max, T):

@@ -57,7 +57,7 @@ struct __align__(16) ShellPair {
   int sa, sb;     // shell indices (for same-shell degeneracy)
   int atom_a, atom_b;
   int comp;       // reference composite index si(si+1)/2+sj, si>=sj
-  int pad;
+  int mol;        // molecule of a batched context (0 for a single geometry)
 };
 
 // Unit of work for one warp: one bra pair against up to 32 consecutive ket
@@ -98,6 +98,8 @@ struct JKArgs {
   double mixed_cutoff;
   unsigned long long* fp32_count;
   int* next_task;             // work counter (zeroed before the launch)
+  const long long* mol_base;  // per molecule: offset of its nbf x nbf block in D, J, K
+  const int* mol_n;           // per molecule: nbf (row stride of its block)
 };
 
 struct StoreArgs {
@@ -126,6 +128,8 @@ struct GradArgs {
   int natoms;        // gradient rows; accumulated per block in shared memory when gsmem
   int gsmem;
   int* next_task;    // work counter (zeroed before the launch)
+  const long long* mol_base;  // per molecule: offset of its block in D
+  const int* mol_n;           // per molecule: nbf
 };
 
 struct OneEArgs {
@@ -150,9 +154,19 @@ cudaError_t launch_store(int X, int Y, const StoreArgs& a, cudaStream_t st);
 cudaError_t launch_grad(int X, int Y, const GradArgs& a, cudaStream_t st);
 cudaError_t launch_schwarz(int X, ShellPair* pairs, const PrimPair* pp, const int* list, int n,
                            double thr, cudaStream_t st);
-cudaError_t launch_scale_density(const double* D, const double* ang, int n, double* Ds, cudaStream_t st);
-cudaError_t launch_symmetrize(const double* X, const double* ang, int n, double* out, cudaStream_t st);
-cudaError_t launch_fock(const double* H, const double* Jt, const double* Kt, const double* ang, int n,
+// Packed per-molecule matrices: molecule m owns elements [base[m], base[m+1])
+// as an n[m] x n[m] row-major block; its basis functions start at bf0[m] in
+// the global angular-factor array.
+struct Packing {
+  const long long* base;  // nmol + 1 offsets (device)
+  const int* n;           // nmol (device)
+  const int* bf0;         // nmol (device)
+  int nmol;
+  long long total;
+};
+cudaError_t launch_scale_density(const double* D, const double* ang, const Packing& P, double* Ds, cudaStream_t st);
+cudaError_t launch_symmetrize(const double* X, const double* ang, const Packing& P, double* out, cudaStream_t st);
+cudaError_t launch_fock(const double* H, const double* Jt, const double* Kt, const double* ang, const Packing& P,
                         double kscale, double* F, cudaStream_t st);
 cudaError_t launch_boys_batch(int m, int n, const double* T, double* F, cudaStream_t st);
 cudaError_t launch_rys_batch(int nr, int n, const double* T, double* R, double* W, cudaStream_t st);

@@ -7,32 +7,49 @@ namespace iqcp {
 
 // ---------------------------------------------------------------------------
 // Element-wise helpers
-__global__ void scale_density_kernel(const double* __restrict__ D, const double* __restrict__ ang,
-                                     int n, double* __restrict__ Ds) {
-  const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (idx >= (long long)n * n) return;
-  const int i = int(idx / n), j = int(idx % n);
-  Ds[idx] = ang[i] * D[idx] * ang[j];
+// molecule owning packed element idx (base has nmol + 1 entries)
+__device__ __forceinline__ int packed_molecule(const long long* __restrict__ base, int nmol, long long idx) {
+  int lo = 0, hi = nmol - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (base[mid] <= idx) lo = mid; else hi = mid - 1;
+  }
+  return lo;
 }
 
-// out = ang_i ang_j (X_ij + X_ji)
-__global__ void symmetrize_kernel(const double* __restrict__ X, const double* __restrict__ ang,
-                                  int n, double* __restrict__ out) {
+// Ds = ang_i D_ij ang_j per molecule block
+__global__ void scale_density_kernel(const double* __restrict__ D, const double* __restrict__ ang, Packing P,
+                                     double* __restrict__ Ds) {
   const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (idx >= (long long)n * n) return;
-  const int i = int(idx / n), j = int(idx % n);
-  out[idx] = ang[i] * ang[j] * (X[idx] + X[(long long)j * n + i]);
+  if (idx >= P.total) return;
+  const int m = packed_molecule(P.base, P.nmol, idx);
+  const long long loc = idx - P.base[m];
+  const int n = P.n[m], i = int(loc / n), j = int(loc % n), b = P.bf0[m];
+  Ds[idx] = ang[b + i] * D[idx] * ang[b + j];
 }
 
-// F = H + ang(Jt+Jt^T)ang - 0.5 k ang(Kt+Kt^T)ang
+// out = ang_i ang_j (X_ij + X_ji) per molecule block
+__global__ void symmetrize_kernel(const double* __restrict__ X, const double* __restrict__ ang, Packing P,
+                                  double* __restrict__ out) {
+  const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (idx >= P.total) return;
+  const int m = packed_molecule(P.base, P.nmol, idx);
+  const long long loc = idx - P.base[m];
+  const int n = P.n[m], i = int(loc / n), j = int(loc % n), b = P.bf0[m];
+  out[idx] = ang[b + i] * ang[b + j] * (X[idx] + X[P.base[m] + (long long)j * n + i]);
+}
+
+// F = H + ang(Jt+Jt^T)ang - 0.5 k ang(Kt+Kt^T)ang per molecule block
 __global__ void fock_kernel(const double* __restrict__ H, const double* __restrict__ Jt,
-                            const double* __restrict__ Kt, const double* __restrict__ ang, int n,
+                            const double* __restrict__ Kt, const double* __restrict__ ang, Packing P,
                             double kscale, double* __restrict__ F) {
   const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (idx >= (long long)n * n) return;
-  const int i = int(idx / n), j = int(idx % n);
-  const long long t = (long long)j * n + i;
-  const double s = ang[i] * ang[j];
+  if (idx >= P.total) return;
+  const int m = packed_molecule(P.base, P.nmol, idx);
+  const long long loc = idx - P.base[m];
+  const int n = P.n[m], i = int(loc / n), j = int(loc % n), b = P.bf0[m];
+  const long long t = P.base[m] + (long long)j * n + i;
+  const double s = ang[b + i] * ang[b + j];
   double v = s * (Jt[idx] + Jt[t]);
   if (Kt) v -= 0.5 * kscale * s * (Kt[idx] + Kt[t]);
   F[idx] = H[idx] + v;
@@ -78,17 +95,17 @@ cudaError_t launch_schwarz(int X, ShellPair* pairs, const PrimPair* pp, const in
 
 static inline int nblk(long long n, int b) { return int((n + b - 1) / b); }
 
-cudaError_t launch_scale_density(const double* D, const double* ang, int n, double* Ds, cudaStream_t st) {
-  scale_density_kernel<<<nblk((long long)n * n, 256), 256, 0, st>>>(D, ang, n, Ds);
+cudaError_t launch_scale_density(const double* D, const double* ang, const Packing& P, double* Ds, cudaStream_t st) {
+  scale_density_kernel<<<nblk(P.total, 256), 256, 0, st>>>(D, ang, P, Ds);
   return cudaGetLastError();
 }
-cudaError_t launch_symmetrize(const double* X, const double* ang, int n, double* out, cudaStream_t st) {
-  symmetrize_kernel<<<nblk((long long)n * n, 256), 256, 0, st>>>(X, ang, n, out);
+cudaError_t launch_symmetrize(const double* X, const double* ang, const Packing& P, double* out, cudaStream_t st) {
+  symmetrize_kernel<<<nblk(P.total, 256), 256, 0, st>>>(X, ang, P, out);
   return cudaGetLastError();
 }
-cudaError_t launch_fock(const double* H, const double* Jt, const double* Kt, const double* ang, int n,
+cudaError_t launch_fock(const double* H, const double* Jt, const double* Kt, const double* ang, const Packing& P,
                         double kscale, double* F, cudaStream_t st) {
-  fock_kernel<<<nblk((long long)n * n, 256), 256, 0, st>>>(H, Jt, Kt, ang, n, kscale, F);
+  fock_kernel<<<nblk(P.total, 256), 256, 0, st>>>(H, Jt, Kt, ang, P, kscale, F);
   return cudaGetLastError();
 }
 cudaError_t launch_boys_batch(int m, int n, const double* T, double* F, cudaStream_t st) {

@@ -137,8 +137,10 @@ __global__ void __launch_bounds__(128) jk_team_kernel(JKArgs args) {
   for (int warp = next_task(args.next_task, lane); warp < args.ntasks; warp = next_task(args.next_task, lane)) {
   const QuartetTask task = args.tasks[warp];
   const ShellPair bp = args.pairs[task.bra];
-  const int n = args.nbf;
-  const double* __restrict__ D = args.D;
+  // this task's molecule block (bra and ket pairs always share a molecule)
+  const int n = args.mol_n[bp.mol];
+  const long long mb = args.mol_base[bp.mol];
+  const double* __restrict__ D = args.D + mb;
   const double AB[3] = {bp.A[0] - bp.B[0], bp.A[1] - bp.B[1], bp.A[2] - bp.B[2]};
   __syncwarp();
   for (int i = lane; i < C::NA * C::NB; i += 32)
@@ -190,14 +192,14 @@ __global__ void __launch_bounds__(128) jk_team_kernel(JKArgs args) {
       double v = 0.0;
 #pragma unroll
       for (int cd = 0; cd < C::NC * C::ND; ++cd) v = fma(work[ab * C::NC * C::ND + cd], Dcd[cd], v);
-      atomicAdd(args.J + (bp.oa + ab / C::NB) * n + bp.ob + ab % C::NB, 2.0 * v);
+      atomicAdd((args.J + mb) + (bp.oa + ab / C::NB) * n + bp.ob + ab % C::NB, 2.0 * v);
     }
     // J~_cd += 2 sum_ab I D_ab
     for (int cd = lane; cd < C::NC * C::ND; cd += 32) {
       double v = 0.0;
 #pragma unroll
       for (int ab = 0; ab < C::NA * C::NB; ++ab) v = fma(work[ab * C::NC * C::ND + cd], Dab[ab], v);
-      atomicAdd(args.J + (kp.oa + cd / C::ND) * n + kp.ob + cd % C::ND, 2.0 * v);
+      atomicAdd((args.J + mb) + (kp.oa + cd / C::ND) * n + kp.ob + cd % C::ND, 2.0 * v);
     }
     if (DO_K) {
       // K~_ac += sum_bd I D_bd
@@ -209,7 +211,7 @@ __global__ void __launch_bounds__(128) jk_team_kernel(JKArgs args) {
 #pragma unroll
           for (int d = 0; d < C::ND; ++d)
             v = fma(work[((a * C::NB + b) * C::NC + c) * C::ND + d], Dbd[b * C::ND + d], v);
-        atomicAdd(args.K + (bp.oa + a) * n + kp.oa + c, v);
+        atomicAdd((args.K + mb) + (bp.oa + a) * n + kp.oa + c, v);
       }
       // K~_bc += sum_ad I D_ad
       for (int x = lane; x < C::NB * C::NC; x += 32) {
@@ -220,7 +222,7 @@ __global__ void __launch_bounds__(128) jk_team_kernel(JKArgs args) {
 #pragma unroll
           for (int d = 0; d < C::ND; ++d)
             v = fma(work[((a * C::NB + b) * C::NC + c) * C::ND + d], Dad[a * C::ND + d], v);
-        atomicAdd(args.K + (bp.ob + b) * n + kp.oa + c, v);
+        atomicAdd((args.K + mb) + (bp.ob + b) * n + kp.oa + c, v);
       }
       // K~_ad += sum_bc I D_bc
       for (int x = lane; x < C::NA * C::ND; x += 32) {
@@ -231,7 +233,7 @@ __global__ void __launch_bounds__(128) jk_team_kernel(JKArgs args) {
 #pragma unroll
           for (int c = 0; c < C::NC; ++c)
             v = fma(work[((a * C::NB + b) * C::NC + c) * C::ND + d], Dbc[b * C::NC + c], v);
-        atomicAdd(args.K + (bp.oa + a) * n + kp.ob + d, v);
+        atomicAdd((args.K + mb) + (bp.oa + a) * n + kp.ob + d, v);
       }
       // K~_bd += sum_ac I D_ac
       for (int x = lane; x < C::NB * C::ND; x += 32) {
@@ -242,7 +244,7 @@ __global__ void __launch_bounds__(128) jk_team_kernel(JKArgs args) {
 #pragma unroll
           for (int c = 0; c < C::NC; ++c)
             v = fma(work[((a * C::NB + b) * C::NC + c) * C::ND + d], Dac[a * C::NC + c], v);
-        atomicAdd(args.K + (bp.ob + b) * n + kp.ob + d, v);
+        atomicAdd((args.K + mb) + (bp.ob + b) * n + kp.ob + d, v);
       }
     }
     __syncwarp();
@@ -318,8 +320,10 @@ __global__ void __launch_bounds__(128) grad_team_kernel(GradArgs args) {
   for (int warp = next_task(args.next_task, lane); warp < args.ntasks; warp = next_task(args.next_task, lane)) {
   const QuartetTask task = args.tasks[warp];
   const ShellPair bp = args.pairs[task.bra];
-  const int n = args.nbf;
-  const double* __restrict__ D = args.D;
+  // this task's molecule block (bra and ket pairs always share a molecule)
+  const int n = args.mol_n[bp.mol];
+  const long long mb = args.mol_base[bp.mol];
+  const double* __restrict__ D = args.D + mb;
   const double AB[3] = {bp.A[0] - bp.B[0], bp.A[1] - bp.B[1], bp.A[2] - bp.B[2]};
   __syncwarp();
   for (int i = lane; i < C::NA * C::NB; i += 32)

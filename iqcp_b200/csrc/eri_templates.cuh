@@ -216,8 +216,10 @@ __global__ void __launch_bounds__(128) jk_kernel(JKArgs args) {
   const QuartetTask task = args.tasks[warp];
   const ShellPair bp = args.pairs[task.bra];
   const int grp = lane / G, sub = lane - grp * G;
-  const int n = args.nbf;
-  const double* __restrict__ D = args.D;
+  // this task's molecule block (bra and ket pairs always share a molecule)
+  const int n = args.mol_n[bp.mol];
+  const long long mb = args.mol_base[bp.mol];
+  const double* __restrict__ D = args.D + mb;
   for (int kbase = 0; kbase < task.nket; kbase += NG) {
     const int kk = kbase + grp;
     const bool active = kk < task.nket;
@@ -256,7 +258,7 @@ __global__ void __launch_bounds__(128) jk_kernel(JKArgs args) {
           v *= 2.0 * f;
         }
         v = warp_sum(v);
-        if (lane == 0) atomicAdd(args.J + (bp.oa + a) * n + bp.ob + b, v);
+        if (lane == 0) atomicAdd((args.J + mb) + (bp.oa + a) * n + bp.ob + b, v);
       }
     if (!digest) continue;
     // J~_cd += 2f sum_ab (ab|cd) D_ab
@@ -273,7 +275,7 @@ __global__ void __launch_bounds__(128) jk_kernel(JKArgs args) {
           double v = 0.0;
 #pragma unroll
           for (int ab = 0; ab < C::NA * C::NB; ++ab) v = fma(acc[(ab * C::NC + c) * C::ND + d], dab[ab], v);
-          atomicAdd(args.J + (kp.oa + c) * n + kp.ob + d, 2.0 * f * v);
+          atomicAdd((args.J + mb) + (kp.oa + c) * n + kp.ob + d, 2.0 * f * v);
         }
     }
     if (!DO_K) continue;
@@ -288,7 +290,7 @@ __global__ void __launch_bounds__(128) jk_kernel(JKArgs args) {
 #pragma unroll
           for (int d = 0; d < C::ND; ++d)
             v = fma(acc[((a * C::NB + b) * C::NC + c) * C::ND + d], __ldg(D + (bp.ob + b) * n + kp.ob + d), v);
-        atomicAdd(args.K + (bp.oa + a) * n + kp.oa + c, f * v);
+        atomicAdd((args.K + mb) + (bp.oa + a) * n + kp.oa + c, f * v);
       }
 #pragma unroll
     for (int b = 0; b < C::NB; ++b)
@@ -300,7 +302,7 @@ __global__ void __launch_bounds__(128) jk_kernel(JKArgs args) {
 #pragma unroll
           for (int d = 0; d < C::ND; ++d)
             v = fma(acc[((a * C::NB + b) * C::NC + c) * C::ND + d], __ldg(D + (bp.oa + a) * n + kp.ob + d), v);
-        atomicAdd(args.K + (bp.ob + b) * n + kp.oa + c, f * v);
+        atomicAdd((args.K + mb) + (bp.ob + b) * n + kp.oa + c, f * v);
       }
 #pragma unroll
     for (int a = 0; a < C::NA; ++a)
@@ -312,7 +314,7 @@ __global__ void __launch_bounds__(128) jk_kernel(JKArgs args) {
 #pragma unroll
           for (int c = 0; c < C::NC; ++c)
             v = fma(acc[((a * C::NB + b) * C::NC + c) * C::ND + d], __ldg(D + (bp.ob + b) * n + kp.oa + c), v);
-        atomicAdd(args.K + (bp.oa + a) * n + kp.ob + d, f * v);
+        atomicAdd((args.K + mb) + (bp.oa + a) * n + kp.ob + d, f * v);
       }
 #pragma unroll
     for (int b = 0; b < C::NB; ++b)
@@ -324,7 +326,7 @@ __global__ void __launch_bounds__(128) jk_kernel(JKArgs args) {
 #pragma unroll
           for (int c = 0; c < C::NC; ++c)
             v = fma(acc[((a * C::NB + b) * C::NC + c) * C::ND + d], __ldg(D + (bp.oa + a) * n + kp.oa + c), v);
-        atomicAdd(args.K + (bp.ob + b) * n + kp.ob + d, f * v);
+        atomicAdd((args.K + mb) + (bp.ob + b) * n + kp.ob + d, f * v);
       }
   }
   }  // task loop
@@ -419,8 +421,10 @@ __global__ void __launch_bounds__(128, (LA + LB + LC + LD <= 1) ? 4 : 1) grad_ke
   const QuartetTask task = args.tasks[warp];
   const ShellPair bp = args.pairs[task.bra];
   const int grp = lane / G, sub = lane - grp * G;
-  const int n = args.nbf;
-  const double* __restrict__ D = args.D;
+  // this task's molecule block (bra and ket pairs always share a molecule)
+  const int n = args.mol_n[bp.mol];
+  const long long mb = args.mol_base[bp.mol];
+  const double* __restrict__ D = args.D + mb;
   const double xs = args.xscale;
   const bool ij_same = bp.sa == bp.sb;
   const double AB[3] = {bp.A[0] - bp.B[0], bp.A[1] - bp.B[1], bp.A[2] - bp.B[2]};

@@ -38,7 +38,18 @@ struct iqcp_ctx {
   iqcp_options opt;
   cudaStream_t own_stream = nullptr;
   cudaStream_t stream = nullptr;
-  int nbf = 0, n_shells = 0, n_atoms = 0;
+  int nbf = 0, n_shells = 0, n_atoms = 0;   // totals over the molecules of the context
+  // batched contexts: molecule m owns rows/cols [0, mol_nbf[m]) of the block at
+  // mol_base[m] in every packed matrix (D, J, K, F, H, S) and atoms
+  // [mol_atom0[m], mol_atom0[m+1]) of the gradient
+  int n_mol = 1;
+  std::vector<long long> mol_base;
+  std::vector<int> mol_nbf, mol_bf0, mol_atom0, mol_shell0;
+  long long packed = 0;
+  long long* d_mol_base = nullptr;
+  int* d_mol_n = nullptr;
+  int* d_mol_bf0 = nullptr;
+  Packing pack{};
   std::vector<int> shell_l, shell_off, shell_atom;
   // device tables
   ShellPair* d_pairs = nullptr;
@@ -123,70 +134,72 @@ int basis_id(const char* name) {
 }
 
 // Build class lists and quartet tasks from Schwarz bounds held in ctx->pairs.
-// Each class list is split into buckets of equal primitive-pair count (so the
-// 32 kets of a warp share one primitive-loop length), each bucket sorted by Q
-// descending so that the Schwarz test Q_bra * Q_ket >= thr keeps a prefix of
-// it.  Unique quartets of a class with itself keep ket position <= bra position
-// in the concatenated list.
+// Per molecule, each class list is split into buckets of equal primitive-pair
+// count (so the 32 kets of a warp share one primitive-loop length), each
+// bucket sorted by Q descending so that the Schwarz test Q_bra * Q_ket >= thr
+// keeps a prefix of it.  Unique quartets of a class with itself keep ket
+// position <= bra position.  Tasks never mix molecules; the tasks of one class
+// pair over all molecules form one range (one launch).
 void build_tasks(iqcp_ctx* ctx, std::vector<int>& ket_list, std::vector<QuartetTask>& tasks) {
   const double thr = ctx->opt.schwarz_threshold;
-  ctx->classes.assign(kNumPairClasses, ClassList());
+  const int NC = kNumPairClasses;
+  std::vector<std::vector<int>> lists((size_t)ctx->n_mol * NC);
   for (int i = 0; i < (int)ctx->pairs.size(); ++i) {
     const ShellPair& p = ctx->pairs[i];
-    const int cls = pair_class(ctx->shell_l[p.sa], ctx->shell_l[p.sb]);
-    ctx->classes[cls].pairs.push_back(i);
+    lists[(size_t)p.mol * NC + pair_class(ctx->shell_l[p.sa], ctx->shell_l[p.sb])].push_back(i);
   }
-  ctx->list_offset.assign(kNumPairClasses + 1, 0);
-  std::vector<std::vector<std::pair<int, int>>> buckets(kNumPairClasses);  // [start, end) per class
+  std::vector<int> seg((size_t)ctx->n_mol * NC);
+  std::vector<std::vector<std::pair<int, int>>> buckets((size_t)ctx->n_mol * NC);
   ket_list.clear();
-  for (int c = 0; c < kNumPairClasses; ++c) {
-    auto& v = ctx->classes[c].pairs;
+  for (size_t li = 0; li < lists.size(); ++li) {
+    auto& v = lists[li];
     std::stable_sort(v.begin(), v.end(), [&](int a, int b) {
       const ShellPair &pa = ctx->pairs[a], &pb = ctx->pairs[b];
       if (pa.np != pb.np) return pa.np > pb.np;
       return pa.Q > pb.Q;
     });
-    for (size_t s = 0; s < v.size();) {
-      size_t e = s;
-      while (e < v.size() && ctx->pairs[v[e]].np == ctx->pairs[v[s]].np) ++e;
-      buckets[c].push_back({(int)s, (int)e});
-      s = e;
+    for (size_t s0 = 0; s0 < v.size();) {
+      size_t e0 = s0;
+      while (e0 < v.size() && ctx->pairs[v[e0]].np == ctx->pairs[v[s0]].np) ++e0;
+      buckets[li].push_back({(int)s0, (int)e0});
+      s0 = e0;
     }
-    ctx->list_offset[c] = (int)ket_list.size();
+    seg[li] = (int)ket_list.size();
     ket_list.insert(ket_list.end(), v.begin(), v.end());
   }
-  ctx->list_offset[kNumPairClasses] = (int)ket_list.size();
   tasks.clear();
   ctx->ranges.clear();
   ctx->n_quartets = 0;
-  for (int X = 0; X < kNumPairClasses; ++X)
+  for (int X = 0; X < NC; ++X)
     for (int Y = 0; Y <= X; ++Y) {
-      const auto& LX = ctx->classes[X].pairs;
-      const auto& LY = ctx->classes[Y].pairs;
       TaskRange r{X, Y, (int)tasks.size(), 0, 0, {default_mode(X, Y, 0), default_mode(X, Y, 1)}};
-      for (int b = 0; b < (int)LX.size(); ++b) {
-        const double qb = ctx->pairs[LX[b]].Q;
-        for (const auto& bk : buckets[Y]) {
-          if (X == Y && bk.first > b) break;
-          const int hi_pos = (X == Y) ? std::min(bk.second, b + 1) : bk.second;
-          // prefix of the bucket with qb * qk >= thr
-          int lo = bk.first, hi = hi_pos;
-          while (lo < hi) {
-            const int mid = (lo + hi) / 2;
-            if (qb * ctx->pairs[LY[mid]].Q < thr) hi = mid; else lo = mid + 1;
-          }
-          const int nk = lo - bk.first;
-          ctx->n_quartets += nk;
-          r.quartets += nk;
-          for (int k0 = 0; k0 < nk; k0 += 32) {
-            QuartetTask t;
-            t.bra = LX[b];
-            t.ket0 = ctx->list_offset[Y] + bk.first + k0;
-            t.nket = std::min(32, nk - k0);
-            t.diag = (X == Y) ? 1 : 0;
-            t.bra_pos = ctx->list_offset[X] + b;
-            t.flags = 0;
-            tasks.push_back(t);
+      for (int m = 0; m < ctx->n_mol; ++m) {
+        const size_t lx = (size_t)m * NC + X, ly = (size_t)m * NC + Y;
+        const auto& LX = lists[lx];
+        const auto& LY = lists[ly];
+        for (int b = 0; b < (int)LX.size(); ++b) {
+          const double qb = ctx->pairs[LX[b]].Q;
+          for (const auto& bk : buckets[ly]) {
+            if (X == Y && bk.first > b) break;
+            const int hi_pos = (X == Y) ? std::min(bk.second, b + 1) : bk.second;
+            int lo = bk.first, hi = hi_pos;   // prefix of the bucket with qb * qk >= thr
+            while (lo < hi) {
+              const int mid = (lo + hi) / 2;
+              if (qb * ctx->pairs[LY[mid]].Q < thr) hi = mid; else lo = mid + 1;
+            }
+            const int nk = lo - bk.first;
+            ctx->n_quartets += nk;
+            r.quartets += nk;
+            for (int k0 = 0; k0 < nk; k0 += 32) {
+              QuartetTask t;
+              t.bra = LX[b];
+              t.ket0 = seg[ly] + bk.first + k0;
+              t.nket = std::min(32, nk - k0);
+              t.diag = (X == Y) ? 1 : 0;
+              t.bra_pos = seg[lx] + b;
+              t.flags = 0;
+              tasks.push_back(t);
+            }
           }
         }
       }
@@ -242,10 +255,11 @@ int run_ranges(iqcp_ctx* ctx, int kind, F&& launch) {
 
 int run_jk_device(iqcp_ctx* ctx, const double* dD, bool want_k) {
   const int n = ctx->nbf;
-  const size_t bytes = sizeof(double) * (size_t)n * n;
+  const size_t bytes = sizeof(double) * (size_t)ctx->packed;
   ctx->launches_total = 1;
-  CK(launch_scale_density(dD, ctx->d_ang, n, ctx->d_Ds, ctx->stream));
-  ctx->mixed_call = ctx->opt.precision == IQCP_MIXED;
+  CK(launch_scale_density(dD, ctx->d_ang, ctx->pack, ctx->d_Ds, ctx->stream));
+  // the mixed form's per-shell-pair |D| bound is kept for single geometries
+  ctx->mixed_call = ctx->opt.precision == IQCP_MIXED && ctx->n_mol == 1;
   if (ctx->mixed_call) {
     CK(launch_shell_dmax(dD, ctx->d_bint + 3 * ctx->n_shells, ctx->d_bint, ctx->n_shells, n, ctx->d_dmax,
                          ctx->stream));
@@ -272,6 +286,8 @@ int run_jk_device(iqcp_ctx* ctx, const double* dD, bool want_k) {
     a.mixed_cutoff = ctx->opt.mixed_cutoff;
     a.fp32_count = ctx->mixed_call ? ctx->d_fp32 : nullptr;
     a.next_task = ctx->cur_counter;
+    a.mol_base = ctx->d_mol_base;
+    a.mol_n = ctx->d_mol_n;
     return launch_jk(r.X, r.Y, a, ctx->stream);
   });
 }
@@ -348,8 +364,10 @@ int iqcp_basis_build(const char* basis_name, int n_atoms, const int* z, const do
 const char* iqcp_last_error(const iqcp_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
 int iqcp_nbf(const iqcp_ctx* ctx) { return ctx ? ctx->nbf : 0; }
 
-int iqcp_create(const iqcp_basis_desc* b, const iqcp_options* opts, iqcp_ctx** out) {
-  if (!b || !out || b->n_shells <= 0 || b->n_atoms <= 0) return IQCP_ERR_ARG;
+static int create_batch(int nmol, const iqcp_basis_desc* descs, const iqcp_options* opts, iqcp_ctx** out) {
+  if (!descs || !out || nmol <= 0) return IQCP_ERR_ARG;
+  for (int m = 0; m < nmol; ++m)
+    if (descs[m].n_shells <= 0 || descs[m].n_atoms <= 0) return IQCP_ERR_ARG;
   iqcp_ctx* ctx = new iqcp_ctx();
   *out = ctx;
   if (opts) ctx->opt = *opts;
@@ -366,88 +384,128 @@ int iqcp_create(const iqcp_basis_desc* b, const iqcp_options* opts, iqcp_ctx** o
   ctx->stream = ctx->own_stream;
   CK(cudaEventCreate(&ctx->ev0));
   CK(cudaEventCreate(&ctx->ev1));
-
-  ctx->n_shells = b->n_shells;
-  ctx->n_atoms = b->n_atoms;
-  std::vector<int> pstart(b->n_shells + 1, 0);
-  int off = 0;
-  for (int s = 0; s < b->n_shells; ++s) {
-    if (b->l[s] < 0 || b->l[s] > kMaxL) return fail(ctx, IQCP_ERR_ARG, "angular momentum above d");
-    if (b->nprim[s] <= 0) return fail(ctx, IQCP_ERR_ARG, "shell without primitives");
-    if (b->atom_of_shell[s] < 0 || b->atom_of_shell[s] >= b->n_atoms) return fail(ctx, IQCP_ERR_ARG, "bad atom index");
-    ctx->shell_l.push_back(b->l[s]);
-    ctx->shell_off.push_back(off);
-    ctx->shell_atom.push_back(b->atom_of_shell[s]);
-    off += ncart(b->l[s]);
-    pstart[s + 1] = pstart[s] + b->nprim[s];
-  }
-  ctx->nbf = off;
-  ctx->n_prims = pstart[b->n_shells];
+  ctx->n_mol = nmol;
   const double kthr = ctx->opt.prim_threshold;
-  for (int s = 0; s < b->n_shells; ++s)
-    for (int d = 0; d < 3; ++d)
-      if (!std::isfinite(b->center[3 * s + d])) return fail(ctx, IQCP_ERR_NUMERIC, "non-finite shell centre");
-  for (int p = 0; p < ctx->n_prims; ++p)
-    if (!(b->exps[p] > 0.0) || !std::isfinite(b->coefs[p])) return fail(ctx, IQCP_ERR_ARG, "bad primitive");
+
+  // concatenate the molecules: global shell, atom, primitive and basis-function
+  // numbering; basis offsets inside a pair stay local to its molecule block
+  std::vector<int> bl, bnp, bps, boff, bz;
+  std::vector<double> bc, bex, bco, bxyz, ang;
+  std::vector<PrimPair> pps;
+  long long base = 0;
+  for (int m = 0; m < nmol; ++m) {
+    const iqcp_basis_desc* b = descs + m;
+    const int s0 = ctx->n_shells, a0 = ctx->n_atoms, p0 = (int)bex.size();
+    ctx->mol_shell0.push_back(s0);
+    ctx->mol_atom0.push_back(a0);
+    ctx->mol_bf0.push_back(ctx->nbf);
+    std::vector<int> pstart(b->n_shells + 1, 0);
+    int off = 0;
+    for (int s = 0; s < b->n_shells; ++s) {
+      if (b->l[s] < 0 || b->l[s] > kMaxL) return fail(ctx, IQCP_ERR_ARG, "angular momentum above d");
+      if (b->nprim[s] <= 0) return fail(ctx, IQCP_ERR_ARG, "shell without primitives");
+      if (b->atom_of_shell[s] < 0 || b->atom_of_shell[s] >= b->n_atoms)
+        return fail(ctx, IQCP_ERR_ARG, "bad atom index");
+      for (int d = 0; d < 3; ++d)
+        if (!std::isfinite(b->center[3 * s + d])) return fail(ctx, IQCP_ERR_NUMERIC, "non-finite shell centre");
+      ctx->shell_l.push_back(b->l[s]);
+      ctx->shell_off.push_back(off);
+      ctx->shell_atom.push_back(a0 + b->atom_of_shell[s]);
+      for (int c = 0; c < ncart(b->l[s]); ++c) ang.push_back(ang_host(b->l[s], c));
+      bl.push_back(b->l[s]);
+      bnp.push_back(b->nprim[s]);
+      bps.push_back(p0 + pstart[s]);
+      boff.push_back(off);
+      for (int d = 0; d < 3; ++d) bc.push_back(b->center[3 * s + d]);
+      off += ncart(b->l[s]);
+      pstart[s + 1] = pstart[s] + b->nprim[s];
+    }
+    for (int p = 0; p < pstart[b->n_shells]; ++p) {
+      if (!(b->exps[p] > 0.0) || !std::isfinite(b->coefs[p])) return fail(ctx, IQCP_ERR_ARG, "bad primitive");
+      bex.push_back(b->exps[p]);
+      bco.push_back(b->coefs[p]);
+    }
+    for (int a = 0; a < b->n_atoms; ++a) {
+      bz.push_back(b->z[a]);
+      for (int d = 0; d < 3; ++d) bxyz.push_back(b->atom_xyz[3 * a + d]);
+    }
+    // shell pairs si >= sj (reference order), A = higher-L shell
+    for (int si = 0; si < b->n_shells; ++si)
+      for (int sj = 0; sj <= si; ++sj) {
+        int sa = si, sb = sj;
+        if (b->l[sj] > b->l[si]) std::swap(sa, sb);
+        ShellPair sp;
+        std::memset(&sp, 0, sizeof(sp));
+        for (int d = 0; d < 3; ++d) {
+          sp.A[d] = b->center[3 * sa + d];
+          sp.B[d] = b->center[3 * sb + d];
+        }
+        sp.sa = s0 + sa;
+        sp.sb = s0 + sb;
+        sp.oa = ctx->shell_off[s0 + sa];
+        sp.ob = ctx->shell_off[s0 + sb];
+        sp.atom_a = a0 + b->atom_of_shell[sa];
+        sp.atom_b = a0 + b->atom_of_shell[sb];
+        sp.comp = si * (si + 1) / 2 + sj;
+        sp.mol = m;
+        sp.pstart = (int)pps.size();
+        double ab2 = 0;
+        for (int d = 0; d < 3; ++d) ab2 += (sp.A[d] - sp.B[d]) * (sp.A[d] - sp.B[d]);
+        for (int i = 0; i < b->nprim[sa]; ++i)
+          for (int j = 0; j < b->nprim[sb]; ++j) {
+            const double ea = b->exps[pstart[sa] + i], eb = b->exps[pstart[sb] + j];
+            const double K = std::exp(-(ea * eb / (ea + eb)) * ab2);
+            if (K < kthr) continue;
+            PrimPair q;
+            q.p = ea + eb;
+            for (int d = 0; d < 3; ++d) q.P[d] = (ea * sp.A[d] + eb * sp.B[d]) / q.p;
+            q.K = K;
+            q.cK = K * b->coefs[pstart[sa] + i] * rad_norm(ea, b->l[sa]) * b->coefs[pstart[sb] + j] *
+                   rad_norm(eb, b->l[sb]);
+            q.aa = ea;
+            q.inv_p = 1.0 / q.p;
+            pps.push_back(q);
+          }
+        sp.np = (int)pps.size() - sp.pstart;
+        ctx->pairs.push_back(sp);
+      }
+    ctx->n_shells += b->n_shells;
+    ctx->n_atoms += b->n_atoms;
+    ctx->nbf += off;
+    ctx->mol_nbf.push_back(off);
+    ctx->mol_base.push_back(base);
+    base += (long long)off * off;
+  }
+  ctx->mol_base.push_back(base);
+  ctx->mol_atom0.push_back(ctx->n_atoms);
+  ctx->mol_shell0.push_back(ctx->n_shells);
+  ctx->packed = base;
+  ctx->n_prims = (int)bex.size();
   {
-    const int ns = b->n_shells, na = b->n_atoms;
     std::vector<int> bi;
-    bi.insert(bi.end(), b->l, b->l + ns);
-    bi.insert(bi.end(), b->nprim, b->nprim + ns);
-    bi.insert(bi.end(), pstart.begin(), pstart.begin() + ns);
-    bi.insert(bi.end(), ctx->shell_off.begin(), ctx->shell_off.end());
-    bi.insert(bi.end(), b->z, b->z + na);
+    bi.insert(bi.end(), bl.begin(), bl.end());
+    bi.insert(bi.end(), bnp.begin(), bnp.end());
+    bi.insert(bi.end(), bps.begin(), bps.end());
+    bi.insert(bi.end(), boff.begin(), boff.end());
+    bi.insert(bi.end(), bz.begin(), bz.end());
     std::vector<double> bd;
-    bd.insert(bd.end(), b->center, b->center + 3 * ns);
-    bd.insert(bd.end(), b->exps, b->exps + ctx->n_prims);
-    bd.insert(bd.end(), b->coefs, b->coefs + ctx->n_prims);
-    bd.insert(bd.end(), b->atom_xyz, b->atom_xyz + 3 * na);
+    bd.insert(bd.end(), bc.begin(), bc.end());
+    bd.insert(bd.end(), bex.begin(), bex.end());
+    bd.insert(bd.end(), bco.begin(), bco.end());
+    bd.insert(bd.end(), bxyz.begin(), bxyz.end());
     CK(cudaMalloc(&ctx->d_bint, sizeof(int) * bi.size()));
     CK(cudaMalloc(&ctx->d_bdbl, sizeof(double) * bd.size()));
     CK(cudaMemcpy(ctx->d_bint, bi.data(), sizeof(int) * bi.size(), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(ctx->d_bdbl, bd.data(), sizeof(double) * bd.size(), cudaMemcpyHostToDevice));
   }
+  CK(cudaMalloc(&ctx->d_mol_base, sizeof(long long) * (nmol + 1)));
+  CK(cudaMalloc(&ctx->d_mol_n, sizeof(int) * nmol));
+  CK(cudaMalloc(&ctx->d_mol_bf0, sizeof(int) * nmol));
+  CK(cudaMemcpy(ctx->d_mol_base, ctx->mol_base.data(), sizeof(long long) * (nmol + 1), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(ctx->d_mol_n, ctx->mol_nbf.data(), sizeof(int) * nmol, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(ctx->d_mol_bf0, ctx->mol_bf0.data(), sizeof(int) * nmol, cudaMemcpyHostToDevice));
+  ctx->pack = Packing{ctx->d_mol_base, ctx->d_mol_n, ctx->d_mol_bf0, nmol, ctx->packed};
 
-  // shell pairs si >= sj (reference order), A = higher-L shell
-  std::vector<PrimPair> pps;
-  for (int si = 0; si < b->n_shells; ++si)
-    for (int sj = 0; sj <= si; ++sj) {
-      int sa = si, sb = sj;
-      if (b->l[sj] > b->l[si]) std::swap(sa, sb);
-      ShellPair sp;
-      std::memset(&sp, 0, sizeof(sp));
-      for (int d = 0; d < 3; ++d) {
-        sp.A[d] = b->center[3 * sa + d];
-        sp.B[d] = b->center[3 * sb + d];
-      }
-      sp.sa = sa;
-      sp.sb = sb;
-      sp.oa = ctx->shell_off[sa];
-      sp.ob = ctx->shell_off[sb];
-      sp.atom_a = b->atom_of_shell[sa];
-      sp.atom_b = b->atom_of_shell[sb];
-      sp.comp = si * (si + 1) / 2 + sj;
-      sp.pstart = (int)pps.size();
-      double ab2 = 0;
-      for (int d = 0; d < 3; ++d) ab2 += (sp.A[d] - sp.B[d]) * (sp.A[d] - sp.B[d]);
-      for (int i = 0; i < b->nprim[sa]; ++i)
-        for (int j = 0; j < b->nprim[sb]; ++j) {
-          const double ea = b->exps[pstart[sa] + i], eb = b->exps[pstart[sb] + j];
-          const double K = std::exp(-(ea * eb / (ea + eb)) * ab2);
-          if (K < kthr) continue;
-          PrimPair q;
-          q.p = ea + eb;
-          for (int d = 0; d < 3; ++d) q.P[d] = (ea * sp.A[d] + eb * sp.B[d]) / q.p;
-          q.K = K;
-          q.cK = K * b->coefs[pstart[sa] + i] * rad_norm(ea, b->l[sa]) * b->coefs[pstart[sb] + j] *
-                 rad_norm(eb, b->l[sb]);
-          q.aa = ea;
-          q.inv_p = 1.0 / q.p;
-          pps.push_back(q);
-        }
-      sp.np = (int)pps.size() - sp.pstart;
-      ctx->pairs.push_back(sp);
-    }
   if (pps.empty()) pps.push_back(PrimPair());
   const int npairs = (int)ctx->pairs.size();
   CK(cudaMalloc(&ctx->d_pairs, sizeof(ShellPair) * npairs));
@@ -485,10 +543,7 @@ int iqcp_create(const iqcp_basis_desc* b, const iqcp_options* opts, iqcp_ctx** o
   CK(cudaMalloc(&ctx->d_tasks, sizeof(QuartetTask) * tasks.size()));
   CK(cudaMemcpy(ctx->d_tasks, tasks.data(), sizeof(QuartetTask) * tasks.size(), cudaMemcpyHostToDevice));
 
-  std::vector<double> ang(ctx->nbf);
-  for (int s = 0; s < b->n_shells; ++s)
-    for (int c = 0; c < ncart(b->l[s]); ++c) ang[ctx->shell_off[s] + c] = ang_host(b->l[s], c);
-  const size_t nn = (size_t)ctx->nbf * ctx->nbf;
+  const size_t nn = (size_t)ctx->packed;
   CK(cudaMalloc(&ctx->d_ang, sizeof(double) * ctx->nbf));
   CK(cudaMemcpy(ctx->d_ang, ang.data(), sizeof(double) * ctx->nbf, cudaMemcpyHostToDevice));
   CK(cudaMalloc(&ctx->d_Ds, sizeof(double) * nn));
@@ -496,10 +551,29 @@ int iqcp_create(const iqcp_basis_desc* b, const iqcp_options* opts, iqcp_ctx** o
   CK(cudaMalloc(&ctx->d_Kt, sizeof(double) * nn));
   for (int i = 0; i < 4; ++i) CK(cudaMalloc(&ctx->d_io[i], sizeof(double) * nn));
   CK(cudaMalloc(&ctx->d_grad, sizeof(double) * 3 * ctx->n_atoms));
-  CK(cudaMalloc(&ctx->d_dmax, sizeof(double) * (size_t)ctx->n_shells * ctx->n_shells));
+  if (nmol == 1) CK(cudaMalloc(&ctx->d_dmax, sizeof(double) * (size_t)ctx->n_shells * ctx->n_shells));
   CK(cudaMalloc(&ctx->d_counters, sizeof(int) * 2 * (ctx->ranges.size() + 1)));
   CK(cudaMalloc(&ctx->d_fp32, sizeof(unsigned long long)));
   return IQCP_OK;
+}
+
+int iqcp_create(const iqcp_basis_desc* b, const iqcp_options* opts, iqcp_ctx** out) {
+  if (!b || !out || b->n_shells <= 0 || b->n_atoms <= 0) return IQCP_ERR_ARG;
+  return create_batch(1, b, opts, out);
+}
+
+int iqcp_create_batch(int n_mol, const iqcp_basis_desc* bases, const iqcp_options* opts, iqcp_ctx** out) {
+  return create_batch(n_mol, bases, opts, out);
+}
+
+int iqcp_batch_layout(const iqcp_ctx* ctx, long long* mat_offset, int* nbf, int* atom_offset) {
+  if (!ctx) return IQCP_ERR_ARG;
+  for (int m = 0; m <= ctx->n_mol; ++m) {
+    if (mat_offset) mat_offset[m] = ctx->mol_base[m];
+    if (atom_offset) atom_offset[m] = ctx->mol_atom0[m];
+    if (nbf && m < ctx->n_mol) nbf[m] = ctx->mol_nbf[m];
+  }
+  return ctx->n_mol;
 }
 
 void iqcp_destroy(iqcp_ctx* ctx) {
@@ -519,6 +593,9 @@ void iqcp_destroy(iqcp_ctx* ctx) {
   cudaFree(ctx->d_bint);
   cudaFree(ctx->d_bdbl);
   cudaFree(ctx->d_dmax);
+  cudaFree(ctx->d_mol_base);
+  cudaFree(ctx->d_mol_n);
+  cudaFree(ctx->d_mol_bf0);
   cudaFree(ctx->d_counters);
   cudaFree(ctx->d_fp32);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
@@ -539,10 +616,10 @@ int iqcp_jk_device(iqcp_ctx* ctx, const double* dD, double* dJ, double* dK) {
   if (rc) return rc;
   rc = run_jk_device(ctx, dD, dK != nullptr);
   if (rc) return rc;
-  CK(launch_symmetrize(ctx->d_Jt, ctx->d_ang, ctx->nbf, dJ, ctx->stream));
+  CK(launch_symmetrize(ctx->d_Jt, ctx->d_ang, ctx->pack, dJ, ctx->stream));
   ctx->launches_total += 1;
   if (dK) {
-    CK(launch_symmetrize(ctx->d_Kt, ctx->d_ang, ctx->nbf, dK, ctx->stream));
+    CK(launch_symmetrize(ctx->d_Kt, ctx->d_ang, ctx->pack, dK, ctx->stream));
     ctx->launches_total += 1;
   }
   return finish_stats(ctx);
@@ -554,7 +631,7 @@ int iqcp_fock_device(iqcp_ctx* ctx, const double* dH, const double* dD, double k
   if (rc) return rc;
   rc = run_jk_device(ctx, dD, k_scale != 0.0);
   if (rc) return rc;
-  CK(launch_fock(dH, ctx->d_Jt, k_scale != 0.0 ? ctx->d_Kt : nullptr, ctx->d_ang, ctx->nbf, k_scale, dF,
+  CK(launch_fock(dH, ctx->d_Jt, k_scale != 0.0 ? ctx->d_Kt : nullptr, ctx->d_ang, ctx->pack, k_scale, dF,
                  ctx->stream));
   ctx->launches_total += 1;
   return finish_stats(ctx);
@@ -604,6 +681,7 @@ static int noalloc_scratch(iqcp_ctx* ctx, double** out) {
 
 int iqcp_jk_device_noalloc(iqcp_ctx* ctx, const double* dD, double* dJ, double* dK) {
   if (!ctx || !dD || !dJ) return IQCP_ERR_ARG;
+  if (ctx->n_mol != 1) return fail(ctx, IQCP_ERR_ARG, "iqcp_jk_device_noalloc takes single-geometry contexts");
   if (ctx->nbf > IQCP_NOALLOC_MAX_NBF)
     return fail(ctx, IQCP_ERR_ARG, "iqcp_jk_device_noalloc supports nbf <= 512 (static scratch size); nbf = " +
                                        std::to_string(ctx->nbf));
@@ -622,7 +700,7 @@ int iqcp_jk_device_noalloc(iqcp_ctx* ctx, const double* dD, double* dJ, double* 
   ctx->profile = false;  // per-launch timing would create events
   ctx->mixed_call = false;
   ctx->launches_total = 1;
-  CK(launch_scale_density(dD, ctx->d_ang, n, Ds, ctx->stream));
+  CK(launch_scale_density(dD, ctx->d_ang, ctx->pack, Ds, ctx->stream));
   CK(cudaMemsetAsync(Jt, 0, sizeof(double) * nn, ctx->stream));
   if (want_k) CK(cudaMemsetAsync(Kt, 0, sizeof(double) * nn, ctx->stream));
   rc = run_ranges(ctx, 0, [&](const TaskRange& r) {
@@ -643,14 +721,16 @@ int iqcp_jk_device_noalloc(iqcp_ctx* ctx, const double* dD, double* dJ, double* 
     a.mixed_cutoff = 0.0;
     a.fp32_count = nullptr;
     a.next_task = ctx->cur_counter;
+    a.mol_base = ctx->d_mol_base;
+    a.mol_n = ctx->d_mol_n;
     return launch_jk(r.X, r.Y, a, ctx->stream);
   });
   ctx->profile = prof;
   if (rc) return rc;
-  CK(launch_symmetrize(Jt, ctx->d_ang, n, dJ, ctx->stream));
+  CK(launch_symmetrize(Jt, ctx->d_ang, ctx->pack, dJ, ctx->stream));
   ctx->launches_total += 1;
   if (want_k) {
-    CK(launch_symmetrize(Kt, ctx->d_ang, n, dK, ctx->stream));
+    CK(launch_symmetrize(Kt, ctx->d_ang, ctx->pack, dK, ctx->stream));
     ctx->launches_total += 1;
   }
   float ms = 0.f;
@@ -664,7 +744,7 @@ int iqcp_jk(iqcp_ctx* ctx, const double* D, double* J, double* K) {
   if (!ctx || !D || !J) return IQCP_ERR_ARG;
   int rc = ensure_device(ctx);
   if (rc) return rc;
-  const size_t bytes = sizeof(double) * (size_t)ctx->nbf * ctx->nbf;
+  const size_t bytes = sizeof(double) * (size_t)ctx->packed;
   CK(cudaMemcpyAsync(ctx->d_io[0], D, bytes, cudaMemcpyHostToDevice, ctx->stream));
   rc = iqcp_jk_device(ctx, ctx->d_io[0], ctx->d_io[1], K ? ctx->d_io[2] : nullptr);
   if (rc) return rc;
@@ -678,7 +758,7 @@ int iqcp_fock(iqcp_ctx* ctx, const double* H, const double* D, double k_scale, d
   if (!ctx || !H || !D || !F) return IQCP_ERR_ARG;
   int rc = ensure_device(ctx);
   if (rc) return rc;
-  const size_t bytes = sizeof(double) * (size_t)ctx->nbf * ctx->nbf;
+  const size_t bytes = sizeof(double) * (size_t)ctx->packed;
   CK(cudaMemcpyAsync(ctx->d_io[0], D, bytes, cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemcpyAsync(ctx->d_io[1], H, bytes, cudaMemcpyHostToDevice, ctx->stream));
   rc = iqcp_fock_device(ctx, ctx->d_io[1], ctx->d_io[0], k_scale, ctx->d_io[2]);
@@ -695,7 +775,7 @@ int iqcp_eri_grad_device(iqcp_ctx* ctx, const double* dD, double hf_frac, double
   const int n = ctx->nbf;
   ctx->launches_total = 1;
   ctx->mixed_call = false;
-  CK(launch_scale_density(dD, ctx->d_ang, n, ctx->d_Ds, ctx->stream));
+  CK(launch_scale_density(dD, ctx->d_ang, ctx->pack, ctx->d_Ds, ctx->stream));
   rc = run_ranges(ctx, 1, [&](const TaskRange& r) {
     GradArgs a;
     a.pairs = ctx->d_pairs;
@@ -713,6 +793,8 @@ int iqcp_eri_grad_device(iqcp_ctx* ctx, const double* dD, double hf_frac, double
     a.gsmem = ctx->n_atoms <= 2048 ? 1 : 0;
     a.mode = r.mode[1];
     a.next_task = ctx->cur_counter;
+    a.mol_base = ctx->d_mol_base;
+    a.mol_n = ctx->d_mol_n;
     return launch_grad(r.X, r.Y, a, ctx->stream);
   });
   if (rc) return rc;
@@ -723,7 +805,7 @@ int iqcp_eri_grad(iqcp_ctx* ctx, const double* D, double hf_frac, double* grad) 
   if (!ctx || !D || !grad) return IQCP_ERR_ARG;
   int rc = ensure_device(ctx);
   if (rc) return rc;
-  const size_t bytes = sizeof(double) * (size_t)ctx->nbf * ctx->nbf;
+  const size_t bytes = sizeof(double) * (size_t)ctx->packed;
   CK(cudaMemcpyAsync(ctx->d_io[0], D, bytes, cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemcpyAsync(ctx->d_grad, grad, sizeof(double) * 3 * ctx->n_atoms, cudaMemcpyHostToDevice, ctx->stream));
   rc = iqcp_eri_grad_device(ctx, ctx->d_io[0], hf_frac, ctx->d_grad);
@@ -735,6 +817,7 @@ int iqcp_eri_grad(iqcp_ctx* ctx, const double* D, double hf_frac, double* grad) 
 
 int iqcp_eri_compressed(iqcp_ctx* ctx, double* out, long long out_len) {
   if (!ctx || !out) return IQCP_ERR_ARG;
+  if (ctx->n_mol != 1) return fail(ctx, IQCP_ERR_ARG, "iqcp_eri_compressed takes single-geometry contexts");
   const long long n = ctx->nbf, np = n * (n + 1) / 2, ne = np * (np + 1) / 2;
   if (out_len < ne) return fail(ctx, IQCP_ERR_ARG, "output too small for the compressed ERI array");
   int rc = ensure_device(ctx);
@@ -765,25 +848,30 @@ int iqcp_one_electron(iqcp_ctx* ctx, double* S, double* T, double* V) {
   if (!ctx) return IQCP_ERR_ARG;
   int rc = ensure_device(ctx);
   if (rc) return rc;
-  const int ns = ctx->n_shells, na = ctx->n_atoms;
-  const size_t bytes = sizeof(double) * (size_t)ctx->nbf * ctx->nbf;
-  OneEArgs a;
-  a.n_shells = ns;
-  a.n_atoms = na;
-  a.nbf = ctx->nbf;
-  a.l = ctx->d_bint;
-  a.nprim = ctx->d_bint + ns;
-  a.pstart = ctx->d_bint + 2 * ns;
-  a.off = ctx->d_bint + 3 * ns;
-  a.z = ctx->d_bint + 4 * ns;
-  a.center = ctx->d_bdbl;
-  a.exps = ctx->d_bdbl + 3 * ns;
-  a.coefs = a.exps + ctx->n_prims;
-  a.atom_xyz = a.coefs + ctx->n_prims;
-  a.S = S ? ctx->d_io[0] : nullptr;
-  a.T = T ? ctx->d_io[1] : nullptr;
-  a.V = V ? ctx->d_io[2] : nullptr;
-  CK(launch_one_electron(a, ctx->stream));
+  const int ns = ctx->n_shells;
+  const size_t bytes = sizeof(double) * (size_t)ctx->packed;
+  // one launch per molecule block of the packed matrices
+  for (int m = 0; m < ctx->n_mol; ++m) {
+    const int s0 = ctx->mol_shell0[m], a0 = ctx->mol_atom0[m];
+    const long long mb = ctx->mol_base[m];
+    OneEArgs a;
+    a.n_shells = ctx->mol_shell0[m + 1] - s0;
+    a.n_atoms = ctx->mol_atom0[m + 1] - a0;
+    a.nbf = ctx->mol_nbf[m];
+    a.l = ctx->d_bint + s0;
+    a.nprim = ctx->d_bint + ns + s0;
+    a.pstart = ctx->d_bint + 2 * ns + s0;
+    a.off = ctx->d_bint + 3 * ns + s0;
+    a.z = ctx->d_bint + 4 * ns + a0;
+    a.center = ctx->d_bdbl + 3 * s0;
+    a.exps = ctx->d_bdbl + 3 * ns;
+    a.coefs = a.exps + ctx->n_prims;
+    a.atom_xyz = a.coefs + ctx->n_prims + 3 * a0;
+    a.S = S ? ctx->d_io[0] + mb : nullptr;
+    a.T = T ? ctx->d_io[1] + mb : nullptr;
+    a.V = V ? ctx->d_io[2] + mb : nullptr;
+    CK(launch_one_electron(a, ctx->stream));
+  }
   if (S) CK(cudaMemcpyAsync(S, ctx->d_io[0], bytes, cudaMemcpyDeviceToHost, ctx->stream));
   if (T) CK(cudaMemcpyAsync(T, ctx->d_io[1], bytes, cudaMemcpyDeviceToHost, ctx->stream));
   if (V) CK(cudaMemcpyAsync(V, ctx->d_io[2], bytes, cudaMemcpyDeviceToHost, ctx->stream));
@@ -840,8 +928,8 @@ int iqcp_autotune(iqcp_ctx* ctx, const double* dD, int reps) {
   if (rc) return rc;
   if (reps < 1) reps = 1;
   const int n = ctx->nbf;
-  const size_t bytes = sizeof(double) * (size_t)n * n;
-  CK(launch_scale_density(dD, ctx->d_ang, n, ctx->d_Ds, ctx->stream));
+  const size_t bytes = sizeof(double) * (size_t)ctx->packed;
+  CK(launch_scale_density(dD, ctx->d_ang, ctx->pack, ctx->d_Ds, ctx->stream));
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
@@ -865,6 +953,7 @@ int iqcp_autotune(iqcp_ctx* ctx, const double* dD, int reps) {
             a.J = ctx->d_Jt; a.K = ctx->d_Kt; a.prim_thr = ctx->opt.prim_threshold; a.mode = mode;
             a.dmax_shell = nullptr; a.n_shells = ctx->n_shells; a.mixed_cutoff = 0.0; a.fp32_count = nullptr;
             a.next_task = ctx->d_counters;
+            a.mol_base = ctx->d_mol_base; a.mol_n = ctx->d_mol_n;
             CK(launch_jk(r.X, r.Y, a, ctx->stream));
           } else {
             GradArgs a;
@@ -875,6 +964,7 @@ int iqcp_autotune(iqcp_ctx* ctx, const double* dD, int reps) {
     a.natoms = ctx->n_atoms;
     a.gsmem = ctx->n_atoms <= 2048 ? 1 : 0; a.mode = mode;
             a.next_task = ctx->d_counters;
+            a.mol_base = ctx->d_mol_base; a.mol_n = ctx->d_mol_n;
             CK(launch_grad(r.X, r.Y, a, ctx->stream));
           }
           CK(cudaEventRecord(e1, ctx->stream));

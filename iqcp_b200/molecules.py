@@ -53,7 +53,9 @@ def generate(n_atoms, heavy_elements, n_heavy, seed, bond=(1.40, 1.55), h_bond=1
                     break
                 j = int(rng.choice(cands))
                 p = pos[j] + _unit(rng) * rng.uniform(*bond)
-                if all(np.linalg.norm(p - pos[k]) >= min_nonbonded for k in range(i) if k != j):
+                d = np.sqrt(((np.asarray(pos) - p) ** 2).sum(axis=1))
+                d[j] = np.inf
+                if np.all(d >= min_nonbonded):
                     pos.append(p)
                     bonds[j] += 1
                     bonds[i] = 1
@@ -71,6 +73,7 @@ def generate(n_atoms, heavy_elements, n_heavy, seed, bond=(1.40, 1.55), h_bond=1
         if (sum(Z) + n_h) % 2:
             n_h = n_h - 1 if n_h > 0 else n_h + 1
         h_pos, h_par = [], []
+        heavy_xyz = np.asarray(pos)
         for _ in range(n_h):
             placed = False
             for _ in range(max_tries):
@@ -79,7 +82,9 @@ def generate(n_atoms, heavy_elements, n_heavy, seed, bond=(1.40, 1.55), h_bond=1
                     break
                 j = int(rng.choice(cands))
                 p = pos[j] + _unit(rng) * h_bond
-                good = all(np.linalg.norm(p - pos[k]) >= min_nonbonded for k in range(n_heavy) if k != j)
+                d = np.sqrt(((heavy_xyz - p) ** 2).sum(axis=1))
+                d[j] = np.inf
+                good = bool(np.all(d >= min_nonbonded))
                 if good:
                     for q, par in zip(h_pos, h_par):
                         lim = min_geminal_hh if par == j else min_nonbonded
@@ -123,13 +128,26 @@ def workload(name, seed=0):
 
 
 def batch_geometries(n=256, seed=0, min_atoms=8, max_atoms=48, displacement=0.1):
-    """Uneven batch: 8-48 atoms from H..Cl, each displaced by up to +-0.1 A."""
+    """Uneven batch: 8-48 atoms from H..Cl, each displaced by up to +-0.1 A.
+
+    Heavy elements C, N, O, F, S, Cl (carbon-rich, so that the trees keep
+    enough free valences); a draw that cannot be placed under the distance
+    rules, or that ends with fewer atoms than drawn, is redrawn from the same
+    seeded stream, so the set is reproducible."""
     rng = np.random.default_rng(seed)
+    heavy = (6, 7, 8, 9, 16, 17)
+    weights = (0.62, 0.12, 0.12, 0.04, 0.06, 0.04)
     out = []
     for g in range(n):
         na = int(rng.integers(min_atoms, max_atoms + 1))
-        nh = max(1, int(round(na * rng.uniform(0.45, 0.6))))
-        atoms = generate(na, (6, 7, 8, 9, 16, 17), nh, int(rng.integers(1 << 30)))
+        while True:
+            nh = max(1, int(round(na * rng.uniform(0.45, 0.6))))
+            try:
+                atoms = generate(na, heavy, nh, int(rng.integers(1 << 30)), max_tries=400, weights=weights)
+            except RuntimeError:
+                continue
+            if len(atoms) >= na - 1:
+                break
         d = rng.uniform(-displacement, displacement, size=(len(atoms), 3)) * ANGSTROM_TO_BOHR
         out.append([(z, tuple(np.array(x) + dx)) for (z, x), dx in zip(atoms, d)])
     return out

@@ -90,3 +90,15 @@ def test_translation_invariance_c2():
     assert np.abs(J1 - J2).max() < 1e-10
     assert np.abs(K1 - K2).max() < 1e-10
     assert np.abs(J1 - J1.T).max() == 0.0 and np.abs(K1 - K1.T).max() == 0.0
+
+
+@pytest.mark.parametrize("mol,basis", SMALL)
+def test_one_electron_vs_oracle(oracle_mod, mol, basis):
+    """Overlap, kinetic and nuclear attraction on the device (integrals/overlap.rs:647,
+    integrals/hcore.rs:103, integrals/nuclear.rs:68-305)."""
+    b = BasisSet.build(REFERENCE_MOLECULES[mol], basis)
+    with FockEngine(b) as eng:
+        S, T, V = eng.one_electron()
+    np.testing.assert_allclose(S, oracle_mod.one_electron(b, "S"), rtol=0, atol=1e-12)
+    np.testing.assert_allclose(T, oracle_mod.one_electron(b, "T"), rtol=0, atol=1e-11)
+    np.testing.assert_allclose(V, oracle_mod.one_electron(b, "V"), rtol=0, atol=1e-10)
