@@ -111,7 +111,10 @@ int iqcp_nbf(const iqcp_ctx* ctx);
 /*
  * Switch the context between the FP64 form and the mixed form (quartets with
  * Q_ij*Q_kl*max|D| below mixed_cutoff run their quadrature in FP32; Rys roots
- * and weights, recurrence coefficients and all accumulation stay FP64).
+ * and weights, recurrence coefficients and all accumulation stay FP64).  max|D|
+ * is the largest density element over the six shell blocks the quartet
+ * digests with; gradients use its square (D x D weights).  Applies to J/K,
+ * Fock and ERI-gradient calls, single or batched contexts.
  */
 int iqcp_set_precision(iqcp_ctx* ctx, int precision, double mixed_cutoff);
 
@@ -133,7 +136,14 @@ int iqcp_jk(iqcp_ctx* ctx, const double* D, double* J, double* K);
  */
 int iqcp_fock(iqcp_ctx* ctx, const double* H, const double* D, double k_scale, double* F);
 
-/* Device-pointer forms of iqcp_jk / iqcp_fock for data resident in HBM. */
+/*
+ * Device-pointer forms of iqcp_jk / iqcp_fock for data resident in HBM.  They
+ * (and iqcp_eri_grad_device, iqcp_one_electron_grad_device) may be captured
+ * into a CUDA graph on the context stream (iqcp_set_stream to the capturing
+ * stream): while the stream captures they only enqueue work, and
+ * iqcp_last_stats / iqcp_launch_profile are not updated.  Call each once
+ * before capturing (the first call sets kernel attributes).
+ */
 int iqcp_jk_device(iqcp_ctx* ctx, const double* d_D, double* d_J, double* d_K);
 int iqcp_fock_device(iqcp_ctx* ctx, const double* d_H, const double* d_D, double k_scale,
                      double* d_F);
@@ -180,6 +190,27 @@ int iqcp_eri_compressed(iqcp_ctx* ctx, double* out, long long out_len);
  */
 int iqcp_one_electron(iqcp_ctx* ctx, double* S, double* T, double* V);
 
+/*
+ * Non-ERI part of the RHF nuclear gradient, added into grad (n_atoms x 3):
+ * nuclear repulsion + sum_mn D_mn dH_mn/dR - sum_mn W_mn dS_mn/dR, with the
+ * Hellmann-Feynman term of the nuclear attraction operator.  W is the
+ * energy-weighted density 2 sum_occ e_i C_mi C_ni (the factor-2 convention of
+ * scf/gradient.rs:116).  Replaces the overlap_derivative_matrix /
+ * hcore_derivative_matrix contractions and the nuclear term of rhf_gradient
+ * (scf/gradient.rs:188, 355, 900-990).  Host buffers, or device pointers for
+ * the _device form (enqueued on the context stream).
+ */
+int iqcp_one_electron_grad(iqcp_ctx* ctx, const double* D, const double* W, double* grad);
+int iqcp_one_electron_grad_device(iqcp_ctx* ctx, const double* d_D, const double* d_W, double* d_grad);
+
+/*
+ * Full RHF nuclear gradient (overwrites grad, n_atoms x 3): the one-electron
+ * part above plus the two-electron part of iqcp_eri_grad with hf_frac = 1.
+ * Replaces rhf_gradient (scf/gradient.rs:900-990), which takes C and the
+ * orbital energies; the caller forms W from them.
+ */
+int iqcp_rhf_gradient(iqcp_ctx* ctx, const double* D, const double* W, double* grad);
+
 /* Schwarz bounds Q[n_shells*n_shells] (compute_schwarz_bounds, eri/mod.rs:1263). */
 int iqcp_schwarz(iqcp_ctx* ctx, double* Q);
 
@@ -201,8 +232,10 @@ int iqcp_last_stats(const iqcp_ctx* ctx, double* stats4);
 /*
  * Measurement support (no counterpart in the reference, which has no GPU path).
  * iqcp_set_profiling: time every quartet-kernel launch with CUDA events.
- * iqcp_launch_profile: per launch of the last call: kind (0 J/K, 1 gradient),
- *   bra/ket pair class, device ms, screened quartets; returns the count.
+ * iqcp_launch_profile: per launch of the last call: kind (0 J/K, 1 gradient,
+ *   2 / 3 their FP32 share in a mixed call), bra/ket pair class, device ms,
+ *   screened quartets of the class (0 for an FP32-share launch); returns the
+ *   count.
  * iqcp_kernel_launches: kernels launched by the last call.
  * iqcp_model_flops: algorithmic FLOPs per (bra class X, ket class Y) [6*6] of
  *   one J/K build (kind 0) or gradient (kind 1), from the closed-form count
@@ -222,9 +255,14 @@ int iqcp_measure_peak(int which, double* tflops);
  * ket class) time each quartet-kernel variant (0: one quartet per thread,
  * 1: one warp per quartet with shared-memory 1D tables) on this device-resident
  * density, best of `reps`, and keep the fastest for J/K and for gradients.
- * Results agree to rounding whichever variant runs.  iqcp_kernel_modes returns
- * the choice as modes[(kind*6 + X)*6 + Y] (-1: class has no quartets);
- * iqcp_set_kernel_mode forces one (X or Y = -1: all classes).
+ * With precision IQCP_MIXED the FP64 and FP32 shares of every class are tuned
+ * separately at the current cutoff, and a class is split into the two only
+ * where that is faster than running it wholly in FP64.  Results agree to
+ * rounding whichever variant runs.  iqcp_kernel_modes fills modes[4*6*6] as
+ * modes[(kind*6 + X)*6 + Y], kind 0 J/K, 1 gradient, 2 / 3 their FP32 share
+ * (-1: class has no quartets; 4 for kinds 2 / 3: the class runs wholly in FP64
+ * in the mixed form); iqcp_set_kernel_mode forces one (kind 0..3, mode 0..3,
+ * or 4 for kinds 2 / 3; X or Y = -1: all classes).
  */
 int iqcp_autotune(iqcp_ctx* ctx, const double* d_D, int reps);
 int iqcp_kernel_modes(const iqcp_ctx* ctx, int* modes);

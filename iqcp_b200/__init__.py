@@ -99,6 +99,10 @@ EXPORTS = {
     "iqcp_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]),
     "iqcp_kernel_modes": (ctypes.c_int, [ctypes.c_void_p, _c_int_p]),
     "iqcp_set_kernel_mode": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "iqcp_one_electron_grad": (ctypes.c_int, [ctypes.c_void_p, _c_dbl_p, _c_dbl_p, _c_dbl_p]),
+    "iqcp_one_electron_grad_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                     ctypes.c_void_p]),
+    "iqcp_rhf_gradient": (ctypes.c_int, [ctypes.c_void_p, _c_dbl_p, _c_dbl_p, _c_dbl_p]),
     "iqcp_create_batch": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_BasisDesc), ctypes.POINTER(_Options),
                                          ctypes.POINTER(ctypes.c_void_p)]),
     "iqcp_batch_layout": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong), _c_int_p, _c_int_p]),
@@ -293,6 +297,20 @@ class FockEngine:
         self._check(self._lib.iqcp_one_electron(self._h, _dp(S), _dp(T), _dp(V)))
         return S, T, V
 
+    def one_electron_gradient(self, D, W):
+        """Nuclear repulsion + sum D dH - sum W dS (W: energy-weighted density, factor 2)."""
+        D, W = self._mat(D), self._mat(W)
+        g = np.zeros((self.basis.n_atoms, 3))
+        self._check(self._lib.iqcp_one_electron_grad(self._h, _dp(D), _dp(W), _dp(g)))
+        return g
+
+    def rhf_gradient(self, D, W):
+        """Full RHF nuclear gradient (rhf_gradient, scf/gradient.rs:900-990)."""
+        D, W = self._mat(D), self._mat(W)
+        g = np.zeros((self.basis.n_atoms, 3))
+        self._check(self._lib.iqcp_rhf_gradient(self._h, _dp(D), _dp(W), _dp(g)))
+        return g
+
     def last_stats(self):
         s = np.zeros(4)
         self._check(self._lib.iqcp_last_stats(self._h, _dp(s)))
@@ -309,7 +327,7 @@ class FockEngine:
         q = np.zeros(m, np.int64)
         n = self._lib.iqcp_launch_profile(self._h, m, _ip(kind), _ip(X), _ip(Y), _dp(ms),
                                           q.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong)))
-        return [{"kind": ("jk", "grad")[kind[i]], "cls": "(%s|%s)" % (PAIR_CLASSES[X[i]], PAIR_CLASSES[Y[i]]),
+        return [{"kind": ("jk", "grad", "jk32", "grad32")[kind[i]], "cls": "(%s|%s)" % (PAIR_CLASSES[X[i]], PAIR_CLASSES[Y[i]]),
                  "X": int(X[i]), "Y": int(Y[i]), "ms": float(ms[i]), "quartets": int(q[i])} for i in range(min(n, m))]
 
     def autotune(self, d_D, reps=2):
@@ -318,12 +336,15 @@ class FockEngine:
         return self.kernel_modes()
 
     def kernel_modes(self):
-        m = np.zeros(72, np.int32)
+        """Variant per [kind, X, Y]; kind 0 J/K, 1 gradient, 2 / 3 their FP32 share
+        (mixed form; 4 = the class runs wholly in FP64)."""
+        m = np.zeros(144, np.int32)
         self._check(self._lib.iqcp_kernel_modes(self._h, _ip(m)))
-        return m.reshape(2, 6, 6)
+        return m.reshape(4, 6, 6)
 
     def set_kernel_mode(self, kind, X=-1, Y=-1, mode=0):
-        self._check(self._lib.iqcp_set_kernel_mode(self._h, {"jk": 0, "grad": 1}[kind], X, Y, mode))
+        k = {"jk": 0, "grad": 1, "jk32": 2, "grad32": 3}[kind]
+        self._check(self._lib.iqcp_set_kernel_mode(self._h, k, X, Y, mode))
 
     def kernel_launches(self):
         return self._lib.iqcp_kernel_launches(self._h)
@@ -441,6 +462,18 @@ class BatchFockEngine(FockEngine):
         D = self.pack(Ds)
         g = np.zeros((self.n_atoms, 3))
         self._check(self._lib.iqcp_eri_grad(self._h, _dp(D), float(hf_frac), _dp(g)))
+        return self.split_atoms(g)
+
+    def one_electron_gradient(self, Ds, Ws):
+        D, W = self.pack(Ds), self.pack(Ws)
+        g = np.zeros((self.n_atoms, 3))
+        self._check(self._lib.iqcp_one_electron_grad(self._h, _dp(D), _dp(W), _dp(g)))
+        return self.split_atoms(g)
+
+    def rhf_gradient(self, Ds, Ws):
+        D, W = self.pack(Ds), self.pack(Ws)
+        g = np.zeros((self.n_atoms, 3))
+        self._check(self._lib.iqcp_rhf_gradient(self._h, _dp(D), _dp(W), _dp(g)))
         return self.split_atoms(g)
 
     def one_electron(self):

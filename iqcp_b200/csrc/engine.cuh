@@ -68,7 +68,7 @@ struct QuartetTask {
   int nket;       // 1..32
   int diag;       // 1 when bra and ket lists are the same class (position ket0+i == bra_pos => pair with itself)
   int bra_pos;    // position of the bra in its class list
-  int flags;      // bit0: evaluate in FP32 (mixed precision)
+  int flags;      // reserved (0)
 };
 
 // Dynamic task distribution of the persistent quartet kernels: lane 0 of a
@@ -77,6 +77,47 @@ __device__ __forceinline__ int next_task(int* counter, int lane) {
   int t = 0;
   if (lane == 0) t = atomicAdd(counter, 1);
   return __shfl_sync(0xffffffffu, t, 0);
+}
+
+// Mixed precision.  A mixed call runs a class either wholly in FP64 or twice
+// over the same task list: pass 1 takes the quartets whose bound
+// Q_ij Q_kl Dmax is at or above the cutoff (FP64 quadrature), pass 2 the rest
+// (FP32 quadrature, FP64 roots, weights and accumulation).  Dmax is the
+// largest |D| over the six shell blocks the quartet digests with (J/K) or its
+// square (gradient, whose weights are products of two density elements).
+// Pass 0 takes every quartet.  The split is fixed once per call as a bit mask
+// per task (precision_mask_kernel).
+struct Mixed {
+  const double* dmax;       // per molecule: max |D| per shell block, ns x ns at dbase[m]
+  const long long* dbase;
+  const int* shell0;        // per molecule: first global shell
+  const int* ns;            // per molecule: shell count
+  double cutoff;
+  int pass;                 // 0 all, 1 FP64 share, 2 FP32 share
+  unsigned long long* fp32_count;  // quartets evaluated in pass 2 (may be null)
+  const unsigned* mask;     // per task of the launch: bit k set = ket k runs in FP32 (passes 1, 2)
+};
+
+__device__ __forceinline__ double mixed_dbound(const Mixed& mx, const ShellPair& bp, const ShellPair& kp) {
+  const int m = bp.mol, s0 = mx.shell0[m], ns = mx.ns[m];
+  const double* dm = mx.dmax + mx.dbase[m];
+  const int i = bp.sa - s0, j = bp.sb - s0, k = kp.sa - s0, l = kp.sb - s0;
+  return fmax(fmax(dm[i * ns + j], dm[k * ns + l]),
+              fmax(fmax(dm[i * ns + k], dm[i * ns + l]), fmax(dm[j * ns + k], dm[j * ns + l])));
+}
+
+// Bit mask of a task's kets in this launch's pass.
+__device__ __forceinline__ unsigned task_sel(const Mixed& mx, int task, int nket) {
+  const unsigned all = nket >= 32 ? 0xffffffffu : ((1u << nket) - 1u);
+  if (mx.pass == 0) return all;
+  const unsigned f32 = __ldg(mx.mask + task);
+  return mx.pass == 2 ? (f32 & all) : (all & ~f32);
+}
+
+// Position of the (k+1)-th set bit of mask (k < popc(mask)).
+__device__ __forceinline__ int nth_set_bit(unsigned mask, int k) {
+  for (int i = 0; i < k; ++i) mask &= mask - 1;
+  return __ffs(mask) - 1;
 }
 
 // Kernel argument blocks (passed by value).
@@ -92,11 +133,7 @@ struct JKArgs {
   double* K;         // may be null
   double prim_thr;
   int mode;          // kernel variant: 0 thread per quartet, 1 warp-cooperative, 2/3: 8/32 lanes per quartet
-  // mixed precision (null dmax_shell: all FP64)
-  const double* dmax_shell;   // max |D| per shell-pair block, n_shells x n_shells
-  int n_shells;
-  double mixed_cutoff;
-  unsigned long long* fp32_count;
+  Mixed mx;
   int* next_task;             // work counter (zeroed before the launch)
   const long long* mol_base;  // per molecule: offset of its nbf x nbf block in D, J, K
   const int* mol_n;           // per molecule: nbf (row stride of its block)
@@ -127,6 +164,7 @@ struct GradArgs {
   int mode;          // kernel variant: 0 thread per quartet, 1 warp-cooperative, 2/3: 8/32 lanes per quartet
   int natoms;        // gradient rows; accumulated per block in shared memory when gsmem
   int gsmem;
+  Mixed mx;
   int* next_task;    // work counter (zeroed before the launch)
   const long long* mol_base;  // per molecule: offset of its block in D
   const int* mol_n;           // per molecule: nbf
@@ -146,6 +184,12 @@ struct OneEArgs {
   double* S;  // may be null
   double* T;  // may be null
   double* V;  // may be null
+  // nuclear gradient of the one-electron energy (one_electron_grad_kernel)
+  const int* atom;     // per shell: atom index
+  const double* D;     // density, nbf x nbf
+  const double* W;     // energy-weighted density (factor 2 convention), nbf x nbf
+  double* grad;        // n_atoms x 3, added to
+  int gsmem;           // accumulate per block in shared memory (3 * n_atoms doubles)
 };
 
 // Host launchers (eri_aux.cu, onee.cu)
@@ -171,8 +215,13 @@ cudaError_t launch_fock(const double* H, const double* Jt, const double* Kt, con
 cudaError_t launch_boys_batch(int m, int n, const double* T, double* F, cudaStream_t st);
 cudaError_t launch_rys_batch(int nr, int n, const double* T, double* R, double* W, cudaStream_t st);
 cudaError_t launch_one_electron(const OneEArgs& a, cudaStream_t st);
-cudaError_t launch_shell_dmax(const double* D, const int* shell_off, const int* shell_l, int n_shells, int nbf,
-                              double* dmax, cudaStream_t st);
+cudaError_t launch_one_electron_grad(const OneEArgs& a, cudaStream_t st);
+// max |D| per shell block of every molecule (layout of Mixed::dmax); D packed
+cudaError_t launch_shell_dmax(const double* D, const Packing& P, const int* shell_off, const int* shell_l,
+                              const Mixed& mx, long long total, double* dmax, cudaStream_t st);
+// FP32 masks of the mixed form for every task (GRAD: density bound squared)
+cudaError_t launch_precision_masks(const ShellPair* pairs, const int* ket_list, const QuartetTask* tasks,
+                                   int ntasks, const Mixed& mx, bool grad, unsigned* mask, cudaStream_t st);
 cudaError_t launch_count_prim_quartets(const ShellPair* pairs, const PrimPair* pp, const int* ket_list,
                                        const QuartetTask* tasks, int ntasks, double thr,
                                        unsigned long long* out, cudaStream_t st);

@@ -118,23 +118,57 @@ cudaError_t launch_rys_batch(int nr, int n, const double* T, double* R, double* 
 }
 
 
-// max |D| over each shell-pair block (mixed-precision quartet bound)
-__global__ void shell_dmax_kernel(const double* __restrict__ D, const int* __restrict__ off,
-                                  const int* __restrict__ l, int ns, int nbf, double* __restrict__ out) {
-  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= ns * ns) return;
-  const int a = idx / ns, b = idx % ns;
-  const int na = ncart(l[a]), nb = ncart(l[b]);
-  double m = 0.0;
+// max |D| over each shell block of every molecule (mixed-precision quartet
+// bound): entry dbase[m] + i * ns[m] + j for local shells i, j of molecule m
+__global__ void shell_dmax_kernel(const double* __restrict__ D, Packing P, const int* __restrict__ off,
+                                  const int* __restrict__ l, Mixed mx, long long total, double* __restrict__ out) {
+  const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (idx >= total) return;
+  const int m = packed_molecule(mx.dbase, P.nmol, idx);
+  const long long loc = idx - mx.dbase[m];
+  const int ns = mx.ns[m], a = mx.shell0[m] + int(loc / ns), b = mx.shell0[m] + int(loc % ns);
+  const int na = ncart(l[a]), nb = ncart(l[b]), n = P.n[m];
+  const double* Dm = D + P.base[m];
+  double v = 0.0;
   for (int i = 0; i < na; ++i)
-    for (int j = 0; j < nb; ++j) m = fmax(m, fabs(D[(long long)(off[a] + i) * nbf + off[b] + j]));
-  out[idx] = m;
+    for (int j = 0; j < nb; ++j) v = fmax(v, fabs(Dm[(long long)(off[a] + i) * n + off[b] + j]));
+  out[idx] = v;
 }
 
-cudaError_t launch_shell_dmax(const double* D, const int* shell_off, const int* shell_l, int n_shells, int nbf,
-                              double* dmax, cudaStream_t st) {
-  const int n = n_shells * n_shells;
-  shell_dmax_kernel<<<(n + 127) / 128, 128, 0, st>>>(D, shell_off, shell_l, n_shells, nbf, dmax);
+cudaError_t launch_shell_dmax(const double* D, const Packing& P, const int* shell_off, const int* shell_l,
+                              const Mixed& mx, long long total, double* dmax, cudaStream_t st) {
+  shell_dmax_kernel<<<nblk(total, 128), 128, 0, st>>>(D, P, shell_off, shell_l, mx, total, dmax);
+  return cudaGetLastError();
+}
+
+// Mixed form: one warp per task, one lane per ket; bit k of mask[task] is set
+// when ket k of the task runs its quadrature in FP32.
+template <bool GRAD>
+__global__ void precision_mask_kernel(const ShellPair* __restrict__ pairs, const int* __restrict__ ket_list,
+                                      const QuartetTask* __restrict__ tasks, int ntasks, Mixed mx,
+                                      unsigned* __restrict__ mask) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= ntasks) return;
+  const QuartetTask t = tasks[warp];
+  bool f32 = false;
+  if (lane < t.nket) {
+    const ShellPair& bp = pairs[t.bra];
+    const ShellPair& kp = pairs[ket_list[t.ket0 + lane]];
+    double d = mixed_dbound(mx, bp, kp);
+    if (GRAD) d *= d;
+    f32 = bp.Q * kp.Q * d < mx.cutoff;
+  }
+  const unsigned m = __ballot_sync(0xffffffffu, f32);
+  if (lane == 0) mask[warp] = m;
+}
+
+cudaError_t launch_precision_masks(const ShellPair* pairs, const int* ket_list, const QuartetTask* tasks,
+                                   int ntasks, const Mixed& mx, bool grad, unsigned* mask, cudaStream_t st) {
+  if (ntasks == 0) return cudaSuccess;
+  const int blocks = (ntasks + 3) / 4;
+  if (grad) precision_mask_kernel<true><<<blocks, 128, 0, st>>>(pairs, ket_list, tasks, ntasks, mx, mask);
+  else precision_mask_kernel<false><<<blocks, 128, 0, st>>>(pairs, ket_list, tasks, ntasks, mx, mask);
   return cudaGetLastError();
 }
 

@@ -1,6 +1,14 @@
-// Instantiation of the grad quartet kernels for bra class (ds|
+// Generated by gen_inst.py: grad dispatch for bra class (ds|
 #include "eri_launch.cuh"
 
 namespace iqcp {
+extern template cudaError_t launch_grad_variant<double, 2, 0, 0, 0>(const GradArgs&, cudaStream_t);
+extern template cudaError_t launch_grad_variant<double, 2, 0, 1, 0>(const GradArgs&, cudaStream_t);
+extern template cudaError_t launch_grad_variant<double, 2, 0, 1, 1>(const GradArgs&, cudaStream_t);
+extern template cudaError_t launch_grad_variant<double, 2, 0, 2, 0>(const GradArgs&, cudaStream_t);
+extern template cudaError_t launch_grad_variant<float, 2, 0, 0, 0>(const GradArgs&, cudaStream_t);
+extern template cudaError_t launch_grad_variant<float, 2, 0, 1, 0>(const GradArgs&, cudaStream_t);
+extern template cudaError_t launch_grad_variant<float, 2, 0, 1, 1>(const GradArgs&, cudaStream_t);
+extern template cudaError_t launch_grad_variant<float, 2, 0, 2, 0>(const GradArgs&, cudaStream_t);
 template cudaError_t launch_grad_bra<2, 0>(int, const GradArgs&, cudaStream_t);
 }  // namespace iqcp

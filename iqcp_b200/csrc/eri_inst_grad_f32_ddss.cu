@@ -1,0 +1,6 @@
+// Generated by gen_inst.py: grad f32 kernels for (dd|ss)
+#include "eri_launch.cuh"
+
+namespace iqcp {
+template cudaError_t launch_grad_variant<float, 2, 2, 0, 0>(const GradArgs&, cudaStream_t);
+}  // namespace iqcp

@@ -1,0 +1,6 @@
+// Generated by gen_inst.py: grad f64 kernels for (pp|pp)
+#include "eri_launch.cuh"
+
+namespace iqcp {
+template cudaError_t launch_grad_variant<double, 1, 1, 1, 1>(const GradArgs&, cudaStream_t);
+}  // namespace iqcp

@@ -1,6 +1,10 @@
-// Instantiation of the grad quartet kernels for bra class (ps|
+// Generated by gen_inst.py: grad dispatch for bra class (ps|
 #include "eri_launch.cuh"
 
 namespace iqcp {
+extern template cudaError_t launch_grad_variant<double, 1, 0, 0, 0>(const GradArgs&, cudaStream_t);
+extern template cudaError_t launch_grad_variant<double, 1, 0, 1, 0>(const GradArgs&, cudaStream_t);
+extern template cudaError_t launch_grad_variant<float, 1, 0, 0, 0>(const GradArgs&, cudaStream_t);
+extern template cudaError_t launch_grad_variant<float, 1, 0, 1, 0>(const GradArgs&, cudaStream_t);
 template cudaError_t launch_grad_bra<1, 0>(int, const GradArgs&, cudaStream_t);
 }  // namespace iqcp

@@ -1,0 +1,6 @@
+// Generated by gen_inst.py: jk f32 kernels for (ds|ss)
+#include "eri_launch.cuh"
+
+namespace iqcp {
+template cudaError_t launch_jk_variant<float, 2, 0, 0, 0>(const JKArgs&, cudaStream_t);
+}  // namespace iqcp

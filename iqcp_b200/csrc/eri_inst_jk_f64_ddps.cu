@@ -1,0 +1,6 @@
+// Generated by gen_inst.py: jk f64 kernels for (dd|ps)
+#include "eri_launch.cuh"
+
+namespace iqcp {
+template cudaError_t launch_jk_variant<double, 2, 2, 1, 0>(const JKArgs&, cudaStream_t);
+}  // namespace iqcp

@@ -1,6 +1,12 @@
-// Instantiation of the jk quartet kernels for bra class (pp|
+// Generated by gen_inst.py: jk dispatch for bra class (pp|
 #include "eri_launch.cuh"
 
 namespace iqcp {
+extern template cudaError_t launch_jk_variant<double, 1, 1, 0, 0>(const JKArgs&, cudaStream_t);
+extern template cudaError_t launch_jk_variant<double, 1, 1, 1, 0>(const JKArgs&, cudaStream_t);
+extern template cudaError_t launch_jk_variant<double, 1, 1, 1, 1>(const JKArgs&, cudaStream_t);
+extern template cudaError_t launch_jk_variant<float, 1, 1, 0, 0>(const JKArgs&, cudaStream_t);
+extern template cudaError_t launch_jk_variant<float, 1, 1, 1, 0>(const JKArgs&, cudaStream_t);
+extern template cudaError_t launch_jk_variant<float, 1, 1, 1, 1>(const JKArgs&, cudaStream_t);
 template cudaError_t launch_jk_bra<1, 1>(int, const JKArgs&, cudaStream_t);
 }  // namespace iqcp

@@ -1,6 +1,10 @@
-// Instantiation of the jk quartet kernels for bra class (ps|
+// Generated by gen_inst.py: jk dispatch for bra class (ps|
 #include "eri_launch.cuh"
 
 namespace iqcp {
+extern template cudaError_t launch_jk_variant<double, 1, 0, 0, 0>(const JKArgs&, cudaStream_t);
+extern template cudaError_t launch_jk_variant<double, 1, 0, 1, 0>(const JKArgs&, cudaStream_t);
+extern template cudaError_t launch_jk_variant<float, 1, 0, 0, 0>(const JKArgs&, cudaStream_t);
+extern template cudaError_t launch_jk_variant<float, 1, 0, 1, 0>(const JKArgs&, cudaStream_t);
 template cudaError_t launch_jk_bra<1, 0>(int, const JKArgs&, cudaStream_t);
 }  // namespace iqcp

@@ -1,4 +1,4 @@
-// Instantiation of the store quartet kernels for bra class (dp|
+// Generated by gen_inst.py: store kernels for bra class (dp|
 #include "eri_launch.cuh"
 
 namespace iqcp {

@@ -1,4 +1,4 @@
-// Instantiation of the store quartet kernels for bra class (ds|
+// Generated by gen_inst.py: store kernels for bra class (ds|
 #include "eri_launch.cuh"
 
 namespace iqcp {

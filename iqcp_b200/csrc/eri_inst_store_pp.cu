@@ -1,4 +1,4 @@
-// Instantiation of the store quartet kernels for bra class (pp|
+// Generated by gen_inst.py: store kernels for bra class (pp|
 #include "eri_launch.cuh"
 
 namespace iqcp {

@@ -1,4 +1,4 @@
-// Instantiation of the store quartet kernels for bra class (ps|
+// Generated by gen_inst.py: store kernels for bra class (ps|
 #include "eri_launch.cuh"
 
 namespace iqcp {

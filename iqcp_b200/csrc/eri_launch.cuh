@@ -36,50 +36,80 @@ inline int persistent_blocks(K kernel, size_t smem, int ntasks) {
 
 // mode: 0 one quartet per thread, 1 warp-cooperative (eri_team.cuh),
 // 2 / 3 eight / thirty-two lanes share one quartet's primitive quartets
-// (small classes only; larger classes fall back to mode 0)
-template <int LA, int LB, int LC, int LD>
-cudaError_t launch_jk_class(const JKArgs& a, cudaStream_t st) {
+// (small classes only; larger classes fall back to mode 0).  The FP32 share
+// of a mixed call (pass 2) has modes 0 (up to 324 components), 1, and 2 for
+// the small classes; other requests map onto those.
+template <typename R, int LA, int LB, int LC, int LD>
+cudaError_t launch_jk_variant(const JKArgs& a, cudaStream_t st) {
   using C = Cls<LA, LB, LC, LD>;
+  constexpr bool F32 = sizeof(R) == 4;
   const size_t tb = sizeof(double) * rys_tab_doubles<C::NR>();
-  if (a.mode == 1) {
+  const bool team = a.mode == 1 || (F32 && C::NCOMP > 324);
+  if (team) {
     const size_t bytes = sizeof(double) * 4 * TeamJK<LA, LB, LC, LD>::PER_WARP + tb;
-    if (a.K) IQCP_LAUNCH((jk_team_kernel<LA, LB, LC, LD, true>), bytes, a, st);
-    else IQCP_LAUNCH((jk_team_kernel<LA, LB, LC, LD, false>), bytes, a, st);
+    if (a.K) IQCP_LAUNCH((jk_team_kernel<R, LA, LB, LC, LD, true>), bytes, a, st);
+    else IQCP_LAUNCH((jk_team_kernel<R, LA, LB, LC, LD, false>), bytes, a, st);
   } else if (C::NCOMP <= 27 && (a.mode == 2 || a.mode == 3)) {
     if constexpr (C::NCOMP <= 27) {
-      if (a.mode == 2) {
-        if (a.K) IQCP_LAUNCH((jk_kernel<LA, LB, LC, LD, 8, true>), tb, a, st);
-        else IQCP_LAUNCH((jk_kernel<LA, LB, LC, LD, 8, false>), tb, a, st);
+      if (a.mode == 2 || F32) {
+        if (a.K) IQCP_LAUNCH((jk_kernel<R, LA, LB, LC, LD, 8, true>), tb, a, st);
+        else IQCP_LAUNCH((jk_kernel<R, LA, LB, LC, LD, 8, false>), tb, a, st);
       } else {
-        if (a.K) IQCP_LAUNCH((jk_kernel<LA, LB, LC, LD, 32, true>), tb, a, st);
-        else IQCP_LAUNCH((jk_kernel<LA, LB, LC, LD, 32, false>), tb, a, st);
+        if (a.K) IQCP_LAUNCH((jk_kernel<R, LA, LB, LC, LD, 32, true>), tb, a, st);
+        else IQCP_LAUNCH((jk_kernel<R, LA, LB, LC, LD, 32, false>), tb, a, st);
       }
     }
-  } else {
-    if (a.K) IQCP_LAUNCH((jk_kernel<LA, LB, LC, LD, 1, true>), tb, a, st);
-    else IQCP_LAUNCH((jk_kernel<LA, LB, LC, LD, 1, false>), tb, a, st);
+  } else if constexpr (!F32 || C::NCOMP <= 324) {
+    if (a.K) IQCP_LAUNCH((jk_kernel<R, LA, LB, LC, LD, 1, true>), tb, a, st);
+    else IQCP_LAUNCH((jk_kernel<R, LA, LB, LC, LD, 1, false>), tb, a, st);
+  }
+  return cudaGetLastError();
+}
+
+template <int LA, int LB, int LC, int LD>
+cudaError_t launch_jk_class(const JKArgs& a, cudaStream_t st) {
+  if (a.mx.pass == 2) return launch_jk_variant<float, LA, LB, LC, LD>(a, st);
+  return launch_jk_variant<double, LA, LB, LC, LD>(a, st);
+}
+
+inline size_t max_smem_optin() {
+  int dev = 0, v = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  return (size_t)v;
+}
+
+template <typename R, int LA, int LB, int LC, int LD>
+cudaError_t launch_grad_variant(const GradArgs& args, cudaStream_t st) {
+  using C = Cls<LA, LB, LC, LD>;
+  constexpr bool F32 = sizeof(R) == 4;
+  constexpr int NRG = (LA + LB + LC + LD + 2) / 2 + 1;
+  const bool team = args.mode == 1 || (F32 && C::NCOMP > 324);
+  const size_t fixed = sizeof(double) * rys_tab_doubles<NRG>() +
+                       (team ? sizeof(double) * 4 * TeamGrad<LA, LB, LC, LD>::PER_WARP : 0);
+  // the per-block gradient accumulator only when it fits beside the tables
+  GradArgs a = args;
+  if (a.gsmem && fixed + sizeof(double) * 3 * a.natoms > max_smem_optin()) a.gsmem = 0;
+  const size_t gacc = a.gsmem ? sizeof(double) * 3 * a.natoms : 0;
+  const size_t tb = sizeof(double) * rys_tab_doubles<NRG>() + gacc;
+  if (team) {
+    const size_t bytes = sizeof(double) * 4 * TeamGrad<LA, LB, LC, LD>::PER_WARP + tb;
+    IQCP_LAUNCH((grad_team_kernel<R, LA, LB, LC, LD>), bytes, a, st);
+  } else if (C::NCOMP <= 36 && (a.mode == 2 || a.mode == 3)) {
+    if constexpr (C::NCOMP <= 36) {
+      if (a.mode == 2 || F32) IQCP_LAUNCH((grad_kernel<R, LA, LB, LC, LD, 8>), tb, a, st);
+      else IQCP_LAUNCH((grad_kernel<R, LA, LB, LC, LD, 32>), tb, a, st);
+    }
+  } else if constexpr (!F32 || C::NCOMP <= 324) {
+    IQCP_LAUNCH((grad_kernel<R, LA, LB, LC, LD, 1>), tb, a, st);
   }
   return cudaGetLastError();
 }
 
 template <int LA, int LB, int LC, int LD>
 cudaError_t launch_grad_class(const GradArgs& a, cudaStream_t st) {
-  using C = Cls<LA, LB, LC, LD>;
-  constexpr int NRG = (LA + LB + LC + LD + 2) / 2 + 1;
-  const size_t gacc = a.gsmem ? sizeof(double) * 3 * a.natoms : 0;
-  const size_t tb = sizeof(double) * rys_tab_doubles<NRG>() + gacc;
-  if (a.mode == 1) {
-    const size_t bytes = sizeof(double) * 4 * TeamGrad<LA, LB, LC, LD>::PER_WARP + tb;
-    IQCP_LAUNCH((grad_team_kernel<LA, LB, LC, LD>), bytes, a, st);
-  } else if (C::NCOMP <= 36 && (a.mode == 2 || a.mode == 3)) {
-    if constexpr (C::NCOMP <= 36) {
-      if (a.mode == 2) IQCP_LAUNCH((grad_kernel<LA, LB, LC, LD, 8>), tb, a, st);
-      else IQCP_LAUNCH((grad_kernel<LA, LB, LC, LD, 32>), tb, a, st);
-    }
-  } else {
-    IQCP_LAUNCH((grad_kernel<LA, LB, LC, LD, 1>), tb, a, st);
-  }
-  return cudaGetLastError();
+  if (a.mx.pass == 2) return launch_grad_variant<float, LA, LB, LC, LD>(a, st);
+  return launch_grad_variant<double, LA, LB, LC, LD>(a, st);
 }
 
 #define IQCP_KET_DISPATCH(X, Y, MACRO)                \

@@ -99,7 +99,7 @@ __device__ __forceinline__ void team_prim_loop(const JKArgs& args, const ShellPa
   }
 }
 
-template <int LA, int LB, int LC, int LD, bool DO_K>
+template <typename R, int LA, int LB, int LC, int LD, bool DO_K>
 __global__ void __launch_bounds__(128) jk_team_kernel(JKArgs args) {
   using C = Cls<LA, LB, LC, LD>;
   using TM = TeamJK<LA, LB, LC, LD>;
@@ -146,29 +146,18 @@ __global__ void __launch_bounds__(128) jk_team_kernel(JKArgs args) {
   for (int i = lane; i < C::NA * C::NB; i += 32)
     Dab[i] = __ldg(D + (bp.oa + i / C::NB) * n + bp.ob + i % C::NB);
 
+  int nf32 = 0;
+  const unsigned sel = task_sel(args.mx, warp, task.nket);
   for (int kk = 0; kk < task.nket; ++kk) {
+    if (!((sel >> kk) & 1u)) continue;  // another pass's ket (the same on every lane)
     const int kpos = task.ket0 + kk;
     const ShellPair kp = args.pairs[__ldg(args.ket_list + kpos)];
     const double CD[3] = {kp.A[0] - kp.B[0], kp.A[1] - kp.B[1], kp.A[2] - kp.B[2]};
     double acc[CPL];
 #pragma unroll
     for (int m = 0; m < CPL; ++m) acc[m] = 0.0;
-    bool f32 = false;
-    if (args.dmax_shell) {
-      // mixed precision: Schwarz bound x largest |D| this quartet digests with
-      const int ns = args.n_shells;
-      const double* dm = args.dmax_shell;
-      double dmax = fmax(fmax(dm[bp.sa * ns + bp.sb], dm[kp.sa * ns + kp.sb]),
-                         fmax(fmax(dm[bp.sa * ns + kp.sa], dm[bp.sa * ns + kp.sb]),
-                              fmax(dm[bp.sb * ns + kp.sa], dm[bp.sb * ns + kp.sb])));
-      f32 = bp.Q * kp.Q * dmax < args.mixed_cutoff;
-    }
-    if (f32) {
-      team_prim_loop<float, LA, LB, LC, LD>(args, bp, kp, AB, CD, offs, acc, reinterpret_cast<float*>(work), lane, rtab);
-      if (lane == 0 && args.fp32_count) atomicAdd(args.fp32_count, 1ull);
-    } else {
-      team_prim_loop<double, LA, LB, LC, LD>(args, bp, kp, AB, CD, offs, acc, work, lane, rtab);
-    }
+    team_prim_loop<R, LA, LB, LC, LD>(args, bp, kp, AB, CD, offs, acc, reinterpret_cast<R*>(work), lane, rtab);
+    ++nf32;
     // ---- digestion ----
     double f = 1.0;
     if (bp.sa == bp.sb) f *= 0.5;
@@ -249,6 +238,7 @@ __global__ void __launch_bounds__(128) jk_team_kernel(JKArgs args) {
     }
     __syncwarp();
   }
+  if (sizeof(R) == 4 && lane == 0 && args.mx.fp32_count && nf32) atomicAdd(args.mx.fp32_count, (unsigned long long)nf32);
   }  // task loop
 }
 
@@ -273,24 +263,26 @@ struct TeamGrad {
   }
 };
 
-template <int LA, int LB, int LC, int LD>
+template <typename R, int LA, int LB, int LC, int LD>
 __global__ void __launch_bounds__(128) grad_team_kernel(GradArgs args) {
   using C = Cls<LA, LB, LC, LD>;
   using TG = TeamGrad<LA, LB, LC, LD>;
   constexpr int NR = TG::NR, TSZ = TG::TSZ, CPL = TG::CPL;
+  constexpr bool F32 = sizeof(R) == 4;
   extern __shared__ double smem[];
   double* rtab = smem;
   rys_stage_table<NR>(rtab);
   __syncthreads();
   const int wib = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
-  double* tab = smem + rys_tab_doubles<NR>() + wib * TG::PER_WARP;
+  double* wbase = smem + rys_tab_doubles<NR>() + wib * TG::PER_WARP;
+  R* tab = reinterpret_cast<R*>(wbase);  // TAB entries of R (the region is sized for double)
   double* gacc = smem + rys_tab_doubles<NR>() + 4 * TG::PER_WARP;
   if (args.gsmem)
     for (int i = threadIdx.x; i < 3 * args.natoms; i += blockDim.x) gacc[i] = 0.0;
   __syncthreads();
   double* gout = args.gsmem ? gacc : args.grad;
-  double* Dab = tab + TG::TAB;
+  double* Dab = wbase + TG::TAB;
   double* Dcd = Dab + C::NA * C::NB;
   double* Dac = Dcd + C::NC * C::ND;
   double* Dbd = Dac + C::NA * C::NC;
@@ -330,14 +322,18 @@ __global__ void __launch_bounds__(128) grad_team_kernel(GradArgs args) {
     Dab[i] = __ldg(D + (bp.oa + i / C::NB) * n + bp.ob + i % C::NB);
   const bool ij_same = bp.sa == bp.sb;
   const double xs = args.xscale;
+  int nf32 = 0;
+  const unsigned sel = task_sel(args.mx, warp, task.nket);
 
   for (int kk = 0; kk < task.nket; ++kk) {
+    if (!((sel >> kk) & 1u)) continue;  // another pass's ket (the same on every lane)
     const int kpos = task.ket0 + kk;
     const ShellPair kp = args.pairs[__ldg(args.ket_list + kpos)];
     // the reference skips when the Schwarz bound of its bra pair (the larger
     // composite index) is below threshold (gradient.rs:1457-1460)
     const double qref = bp.comp >= kp.comp ? bp.Q : kp.Q;
     if (qref < args.schwarz_thr) continue;
+    ++nf32;
     const bool kl_same = kp.sa == kp.sb;
     const bool bk_same = task.diag && kpos == task.bra_pos;
     for (int i = lane; i < C::NC * C::ND; i += 32) Dcd[i] = __ldg(D + (kp.oa + i / C::ND) * n + kp.ob + i % C::ND);
@@ -397,42 +393,53 @@ __global__ void __launch_bounds__(128) grad_team_kernel(GradArgs args) {
           const double b10 = fma(h, pb.inv_p, b00), b01 = fma(h, pk.inv_p, b00);
           const double pa = pb.P[ax] - bp.A[ax], qc = pk.P[ax] - kp.A[ax];
           const double g00 = ax == 2 ? wr * kTwoPi52 * pb.cK * pk.cK * pb.inv_p * pk.inv_p * inv_s * sqrt(s) : 1.0;
-          axis_table<double, LA + LB + 1, LC + LD + 1, TG::EA, TG::EB, TG::EC, TG::ED>(
-              pa - t2 * q * inv_s * PQ[ax], qc + t2 * p * inv_s * PQ[ax], b00, b10, b01, AB[ax], CD[ax], g00,
-              tab + (r * 3 + ax) * TSZ);
+          axis_table<R, LA + LB + 1, LC + LD + 1, TG::EA, TG::EB, TG::EC, TG::ED>(
+              R(pa - t2 * q * inv_s * PQ[ax]), R(qc + t2 * p * inv_s * PQ[ax]), R(b00), R(b10), R(b01), R(AB[ax]),
+              R(CD[ax]), R(g00), tab + (r * 3 + ax) * TSZ);
         }
         __syncwarp();
-        const double e2[3] = {2.0 * pb.aa, 2.0 * (pb.p - pb.aa), 2.0 * pk.aa};
+        const R e2[3] = {R(2.0 * pb.aa), R(2.0 * (pb.p - pb.aa)), R(2.0 * pk.aa)};
         const int str[3] = {TG::SA, TG::SB, TG::SC};
+        // FP32 share: this primitive quartet's derivatives in R, then added to the FP64 sums
+        R gp[F32 ? 9 : 1];
+        if constexpr (F32) {
+#pragma unroll
+          for (int x = 0; x < 9; ++x) gp[x] = R(0);
+        }
 #pragma unroll
         for (int m = 0; m < CPL; ++m) {
-          const double w = W[m];
-          if (w == 0.0) continue;
+          const R w = R(W[m]);
+          if (W[m] == 0.0) continue;
           const int o = offs[m], pw = pows[m];
 #pragma unroll
           for (int r = 0; r < NR; ++r) {
-            const double* t = tab + r * 3 * TSZ;
+            const R* t = tab + r * 3 * TSZ;
             int ox[3];
-            double reg[3];
+            R reg[3];
 #pragma unroll
             for (int ax = 0; ax < 3; ++ax) {
               ox[ax] = (o >> (10 * ax)) & 0x3ff;
               reg[ax] = t[ox[ax]];
             }
-            const double wyz = w * reg[1] * reg[2], wxz = w * reg[0] * reg[2], wxy = w * reg[0] * reg[1];
-            const double wo[3] = {wyz, wxz, wxy};
+            const R wyz = w * reg[1] * reg[2], wxz = w * reg[0] * reg[2], wxy = w * reg[0] * reg[1];
+            const R wo[3] = {wyz, wxz, wxy};
 #pragma unroll
             for (int ax = 0; ax < 3; ++ax) {
 #pragma unroll
               for (int cen = 0; cen < 3; ++cen) {
                 const int pcen = (pw >> (6 * ax + 2 * cen)) & 3;
-                const double up = t[ox[ax] + str[cen]];
+                const R up = t[ox[ax] + str[cen]];
                 // power 0 has no lowered term; the index is clamped so no load leaves the table
-                const double dn = double(pcen) * t[pcen ? ox[ax] - str[cen] : ox[ax]];
-                g[3 * cen + ax] = fma(wo[ax], e2[cen] * up - dn, g[3 * cen + ax]);
+                const R dn = R(pcen) * t[pcen ? ox[ax] - str[cen] : ox[ax]];
+                if constexpr (F32) gp[3 * cen + ax] = fmaf(wo[ax], e2[cen] * up - dn, gp[3 * cen + ax]);
+                else g[3 * cen + ax] = fma(wo[ax], e2[cen] * up - dn, g[3 * cen + ax]);
               }
             }
           }
+        }
+        if constexpr (F32) {
+#pragma unroll
+          for (int x = 0; x < 9; ++x) g[x] += double(gp[x]);
         }
       }
     }
@@ -451,6 +458,7 @@ __global__ void __launch_bounds__(128) grad_team_kernel(GradArgs args) {
     }
     __syncwarp();
   }
+  if (F32 && lane == 0 && args.mx.fp32_count && nf32) atomicAdd(args.mx.fp32_count, (unsigned long long)nf32);
   }  // task loop
   if (args.gsmem) {
     __syncthreads();

@@ -111,15 +111,19 @@ __device__ __forceinline__ PrimPair load_pp(const PrimPair* __restrict__ p) {
   return r;
 }
 
-// Contracted (radially normalised) quartet (ab|cd) into acc[NCOMP], FP64.
+// Contracted (radially normalised) quartet (ab|cd) into acc[NCOMP].
 // Primitive quartets are visited as items it = i * np_ket + j, starting at
 // `first` with step `stride`, so that `stride` lanes can share one quartet.
-template <int LA, int LB, int LC, int LD>
-__device__ __forceinline__ void quartet_fp64(const ShellPair& bp, const ShellPair& kp,
-                                             const PrimPair* __restrict__ pp, double thr,
-                                             double* __restrict__ acc, int first = 0, int stride = 1,
-                                             const double* rtab = nullptr) {
+// R is the quadrature type: double, or float for the FP32 share of the mixed
+// form, where the roots, weights and recurrence coefficients are formed in
+// FP64 and rounded once, and each primitive quartet's FP32 block is added to
+// the FP64 accumulators.
+template <typename R, int LA, int LB, int LC, int LD>
+__device__ __forceinline__ void quartet(const ShellPair& bp, const ShellPair& kp, const PrimPair* __restrict__ pp,
+                                        double thr, double* __restrict__ acc, int first = 0, int stride = 1,
+                                        const double* rtab = nullptr) {
   using C = Cls<LA, LB, LC, LD>;
+  constexpr bool F32 = sizeof(R) == 4;
 #pragma unroll
   for (int i = 0; i < C::NCOMP; ++i) acc[i] = 0.0;
   const double AB[3] = {bp.A[0] - bp.B[0], bp.A[1] - bp.B[1], bp.A[2] - bp.B[2]};
@@ -137,52 +141,60 @@ __device__ __forceinline__ void quartet_fp64(const ShellPair& bp, const ShellPai
       jl = j;
     }
     const PrimPair b = load_pp(pp + bp.pstart + i);
-    {
-      if (b.K * k.K < thr) continue;
-      const double p = b.p, q = k.p, s = p + q;
-      const double PQ[3] = {b.P[0] - k.P[0], b.P[1] - k.P[1], b.P[2] - k.P[2]};
-      const double inv_s = 1.0 / s;
-        const double rho = p * q * inv_s;
-      const double T = rho * (PQ[0] * PQ[0] + PQ[1] * PQ[1] + PQ[2] * PQ[2]);
-      const double pref = kTwoPi52 * b.cK * k.cK * b.inv_p * k.inv_p * inv_s * sqrt(s);
-      double rt[C::NR], wt[C::NR];
-      if (rtab) rys_rule_tab<C::NR>(T, rtab, rt, wt);
-      else rys_rule<C::NR>(T, rt, wt);
-      const double PA[3] = {b.P[0] - bp.A[0], b.P[1] - bp.A[1], b.P[2] - bp.A[2]};
-      const double QC[3] = {k.P[0] - kp.A[0], k.P[1] - kp.A[1], k.P[2] - kp.A[2]};
+    if (b.K * k.K < thr) continue;
+    const double p = b.p, q = k.p, s = p + q;
+    const double PQ[3] = {b.P[0] - k.P[0], b.P[1] - k.P[1], b.P[2] - k.P[2]};
+    const double inv_s = 1.0 / s;
+    const double rho = p * q * inv_s;
+    const double T = rho * (PQ[0] * PQ[0] + PQ[1] * PQ[1] + PQ[2] * PQ[2]);
+    const double pref = kTwoPi52 * b.cK * k.cK * b.inv_p * k.inv_p * inv_s * sqrt(s);
+    double rt[C::NR], wt[C::NR];
+    if (rtab) rys_rule_tab<C::NR>(T, rtab, rt, wt);
+    else rys_rule<C::NR>(T, rt, wt);
+    const double PA[3] = {b.P[0] - bp.A[0], b.P[1] - bp.A[1], b.P[2] - bp.A[2]};
+    const double QC[3] = {k.P[0] - kp.A[0], k.P[1] - kp.A[1], k.P[2] - kp.A[2]};
+    R part[F32 ? C::NCOMP : 1];
+    if constexpr (F32) {
 #pragma unroll
-      for (int r = 0; r < C::NR; ++r) {
-        const double t2 = rt[r];
-        // rys_coefficients.rs:94-180 with u2 (p+q) + pq = pq / (1 - t^2):
-        // tmp5 = t^2 / (2(p+q)), tmp4 q = (1 - t^2) / (2p), tmp4 p = (1 - t^2) / (2q)
-        const double b00 = 0.5 * t2 * inv_s, h = 0.5 - 0.5 * t2;
-        const double b10 = fma(h, b.inv_p, b00), b01 = fma(h, k.inv_p, b00);
-        const double f2 = t2 * q * inv_s, f3 = t2 * p * inv_s;
-        double Ix[C::TSZ], Iy[C::TSZ], Iz[C::TSZ];
-        axis_table<double, C::NBRA, C::NKET, LA, LB, LC, LD>(
-            PA[0] - f2 * PQ[0], QC[0] + f3 * PQ[0], b00, b10, b01, AB[0], CD[0], 1.0, Ix);
-        axis_table<double, C::NBRA, C::NKET, LA, LB, LC, LD>(
-            PA[1] - f2 * PQ[1], QC[1] + f3 * PQ[1], b00, b10, b01, AB[1], CD[1], 1.0, Iy);
-        axis_table<double, C::NBRA, C::NKET, LA, LB, LC, LD>(
-            PA[2] - f2 * PQ[2], QC[2] + f3 * PQ[2], b00, b10, b01, AB[2], CD[2], wt[r] * pref, Iz);
+      for (int o = 0; o < C::NCOMP; ++o) part[o] = R(0);
+    }
 #pragma unroll
-        for (int a = 0; a < C::NA; ++a)
+    for (int r = 0; r < C::NR; ++r) {
+      const double t2 = rt[r];
+      // rys_coefficients.rs:94-180 with u2 (p+q) + pq = pq / (1 - t^2):
+      // tmp5 = t^2 / (2(p+q)), tmp4 q = (1 - t^2) / (2p), tmp4 p = (1 - t^2) / (2q)
+      const double b00 = 0.5 * t2 * inv_s, h = 0.5 - 0.5 * t2;
+      const double b10 = fma(h, b.inv_p, b00), b01 = fma(h, k.inv_p, b00);
+      const double f2 = t2 * q * inv_s, f3 = t2 * p * inv_s;
+      R Ix[C::TSZ], Iy[C::TSZ], Iz[C::TSZ];
+      axis_table<R, C::NBRA, C::NKET, LA, LB, LC, LD>(R(PA[0] - f2 * PQ[0]), R(QC[0] + f3 * PQ[0]), R(b00), R(b10),
+                                                      R(b01), R(AB[0]), R(CD[0]), R(1), Ix);
+      axis_table<R, C::NBRA, C::NKET, LA, LB, LC, LD>(R(PA[1] - f2 * PQ[1]), R(QC[1] + f3 * PQ[1]), R(b00), R(b10),
+                                                      R(b01), R(AB[1]), R(CD[1]), R(1), Iy);
+      axis_table<R, C::NBRA, C::NKET, LA, LB, LC, LD>(R(PA[2] - f2 * PQ[2]), R(QC[2] + f3 * PQ[2]), R(b00), R(b10),
+                                                      R(b01), R(AB[2]), R(CD[2]), R(wt[r] * pref), Iz);
 #pragma unroll
-          for (int bb = 0; bb < C::NB; ++bb)
+      for (int a = 0; a < C::NA; ++a)
 #pragma unroll
-            for (int c = 0; c < C::NC; ++c)
+        for (int bb = 0; bb < C::NB; ++bb)
 #pragma unroll
-              for (int d = 0; d < C::ND; ++d) {
-                const int ix = C::tidx(cart_pow(LA, a, 0), cart_pow(LB, bb, 0), cart_pow(LC, c, 0),
-                                       cart_pow(LD, d, 0));
-                const int iy = C::tidx(cart_pow(LA, a, 1), cart_pow(LB, bb, 1), cart_pow(LC, c, 1),
-                                       cart_pow(LD, d, 1));
-                const int iz = C::tidx(cart_pow(LA, a, 2), cart_pow(LB, bb, 2), cart_pow(LC, c, 2),
-                                       cart_pow(LD, d, 2));
-                const int o = ((a * C::NB + bb) * C::NC + c) * C::ND + d;
-                acc[o] = fma(Ix[ix] * Iy[iy], Iz[iz], acc[o]);
-              }
-      }
+          for (int c = 0; c < C::NC; ++c)
+#pragma unroll
+            for (int d = 0; d < C::ND; ++d) {
+              const int ix = C::tidx(cart_pow(LA, a, 0), cart_pow(LB, bb, 0), cart_pow(LC, c, 0),
+                                     cart_pow(LD, d, 0));
+              const int iy = C::tidx(cart_pow(LA, a, 1), cart_pow(LB, bb, 1), cart_pow(LC, c, 1),
+                                     cart_pow(LD, d, 1));
+              const int iz = C::tidx(cart_pow(LA, a, 2), cart_pow(LB, bb, 2), cart_pow(LC, c, 2),
+                                     cart_pow(LD, d, 2));
+              const int o = ((a * C::NB + bb) * C::NC + c) * C::ND + d;
+              if constexpr (F32) part[o] = fmaf(Ix[ix] * Iy[iy], Iz[iz], part[o]);
+              else acc[o] = fma(Ix[ix] * Iy[iy], Iz[iz], acc[o]);
+            }
+    }
+    if constexpr (F32) {
+#pragma unroll
+      for (int o = 0; o < C::NCOMP; ++o) acc[o] += double(part[o]);
     }
   }
 }
@@ -204,7 +216,7 @@ __device__ __forceinline__ double group_sum(double v) {
   return v;
 }
 
-template <int LA, int LB, int LC, int LD, int G, bool DO_K>
+template <typename R, int LA, int LB, int LC, int LD, int G, bool DO_K>
 __global__ void __launch_bounds__(128) jk_kernel(JKArgs args) {
   using C = Cls<LA, LB, LC, LD>;
   constexpr int NG = 32 / G;
@@ -220,16 +232,20 @@ __global__ void __launch_bounds__(128) jk_kernel(JKArgs args) {
   const int n = args.mol_n[bp.mol];
   const long long mb = args.mol_base[bp.mol];
   const double* __restrict__ D = args.D + mb;
-  for (int kbase = 0; kbase < task.nket; kbase += NG) {
+  // kets of this pass, compacted so that no group idles on the other pass's kets
+  const unsigned sel = task_sel(args.mx, warp, task.nket);
+  const int nsel = __popc(sel);
+  if (sizeof(R) == 4 && lane == 0 && args.mx.fp32_count && nsel) atomicAdd(args.mx.fp32_count, (unsigned long long)nsel);
+  for (int kbase = 0; kbase < nsel; kbase += NG) {
     const int kk = kbase + grp;
-    const bool active = kk < task.nket;
+    const bool active = kk < nsel;
     double acc[C::NCOMP];
     double f = 0.0;
     ShellPair kp = bp;
     if (active) {
-      const int kpos = task.ket0 + kk;
+      const int kpos = task.ket0 + (args.mx.pass ? nth_set_bit(sel, kk) : kk);
       kp = args.pairs[__ldg(args.ket_list + kpos)];
-      quartet_fp64<LA, LB, LC, LD>(bp, kp, args.pp, args.prim_thr, acc, sub, G, rtab);
+      quartet<R, LA, LB, LC, LD>(bp, kp, args.pp, args.prim_thr, acc, sub, G, rtab);
       f = 1.0;
       if (bp.sa == bp.sb) f *= 0.5;
       if (kp.sa == kp.sb) f *= 0.5;
@@ -344,7 +360,7 @@ __global__ void __launch_bounds__(128) schwarz_kernel(ShellPair* pairs, const Pr
   const int pid = list[t];
   const ShellPair bp = pairs[pid];
   double acc[C::NCOMP];
-  quartet_fp64<LA, LB, LA, LB>(bp, bp, pp, thr, acc);
+  quartet<double, LA, LB, LA, LB>(bp, bp, pp, thr, acc);
   double mx = 0.0;
 #pragma unroll
   for (int a = 0; a < C::NA; ++a)
@@ -378,7 +394,7 @@ __global__ void __launch_bounds__(128) store_kernel(StoreArgs args) {
   const ShellPair bp = args.pairs[task.bra];
   const ShellPair kp = args.pairs[args.ket_list[task.ket0 + lane]];
   double acc[C::NCOMP];
-  quartet_fp64<LA, LB, LC, LD>(bp, kp, args.pp, args.prim_thr, acc);
+  quartet<double, LA, LB, LC, LD>(bp, kp, args.pp, args.prim_thr, acc);
 #pragma unroll
   for (int a = 0; a < C::NA; ++a)
 #pragma unroll
@@ -397,7 +413,7 @@ __global__ void __launch_bounds__(128) store_kernel(StoreArgs args) {
 
 // ---------------------------------------------------------------------------
 // Two-electron gradient (eri_gradient_fused, scf/gradient.rs:1430-1640).
-template <int LA, int LB, int LC, int LD, int G>
+template <typename R, int LA, int LB, int LC, int LD, int G>
 __global__ void __launch_bounds__(128, (LA + LB + LC + LD <= 1) ? 4 : 1) grad_kernel(GradArgs args) {
   using C = Cls<LA, LB, LC, LD>;
   // tables extended by one on A, B, C; the D derivative follows from
@@ -407,6 +423,7 @@ __global__ void __launch_bounds__(128, (LA + LB + LC + LD <= 1) ? 4 : 1) grad_ke
   auto eidx = [](int a, int b, int c, int d) { return ((a * (EB + 1) + b) * (EC + 1) + c) * (ED + 1) + d; };
   constexpr int NR = (LA + LB + LC + LD + 2) / 2 + 1;
   constexpr int NG = 32 / G;
+  constexpr bool F32 = sizeof(R) == 4;
   extern __shared__ double rtab[];
   rys_stage_table<NR>(rtab);
   // per-block gradient accumulator: many quartets hit the same few atoms, so
@@ -429,13 +446,16 @@ __global__ void __launch_bounds__(128, (LA + LB + LC + LD <= 1) ? 4 : 1) grad_ke
   const bool ij_same = bp.sa == bp.sb;
   const double AB[3] = {bp.A[0] - bp.B[0], bp.A[1] - bp.B[1], bp.A[2] - bp.B[2]};
   double gA[3] = {0, 0, 0}, gB[3] = {0, 0, 0};
-  for (int kbase = 0; kbase < task.nket; kbase += NG) {
+  const unsigned sel = task_sel(args.mx, warp, task.nket);
+  const int nsel = __popc(sel);
+  if (F32 && lane == 0 && args.mx.fp32_count && nsel) atomicAdd(args.mx.fp32_count, (unsigned long long)nsel);
+  for (int kbase = 0; kbase < nsel; kbase += NG) {
     const int kk = kbase + grp;
-    bool active = kk < task.nket;
+    bool active = kk < nsel;
     ShellPair kp = bp;
     int kpos = 0;
     if (active) {
-      kpos = task.ket0 + kk;
+      kpos = task.ket0 + (args.mx.pass ? nth_set_bit(sel, kk) : kk);
       kp = args.pairs[__ldg(args.ket_list + kpos)];
       // the reference skips when the Schwarz bound of its bra pair (the larger
       // composite index) is below threshold (gradient.rs:1457-1460)
@@ -446,7 +466,7 @@ __global__ void __launch_bounds__(128, (LA + LB + LC + LD <= 1) ? 4 : 1) grad_ke
     if (active) {
       const bool kl_same = kp.sa == kp.sb;
       const bool bk_same = task.diag && kpos == task.bra_pos;
-      double W[C::NCOMP];
+      R W[C::NCOMP];
 #pragma unroll
       for (int a = 0; a < C::NA; ++a)
 #pragma unroll
@@ -473,14 +493,14 @@ __global__ void __launch_bounds__(128, (LA + LB + LC + LD <= 1) ? 4 : 1) grad_ke
               // D is angular-scaled: t = w_ref * (ang_a ang_b ang_c ang_d); the
               // |w| < 1e-15 skip applies to the reference weight w_ref
               const double angp = ang_factor(LA, a) * ang_factor(LB, b) * ang_factor(LC, c) * ang_factor(LD, d);
-              W[((a * C::NB + b) * C::NC + c) * C::ND + d] = (fabs(t / angp) < 1e-15) ? 0.0 : t;
+              W[((a * C::NB + b) * C::NC + c) * C::ND + d] = R((fabs(t / angp) < 1e-15) ? 0.0 : t);
             }
       const double CD[3] = {kp.A[0] - kp.B[0], kp.A[1] - kp.B[1], kp.A[2] - kp.B[2]};
       const int nitems = bp.np * kp.np;
       int jl = -1;
       PrimPair k;
       for (int it = sub; it < nitems; it += G) {
-        // ket-major order (see quartet_fp64)
+        // ket-major order (see quartet)
         const int pj = it / bp.np, pi = it - pj * bp.np;
         if (pj != jl) {
           k = load_pp(args.pp + kp.pstart + pj);
@@ -498,7 +518,9 @@ __global__ void __launch_bounds__(128, (LA + LB + LC + LD <= 1) ? 4 : 1) grad_ke
         rys_rule_tab<NR>(T, rtab, rt, wt);
         const double PA[3] = {b.P[0] - bp.A[0], b.P[1] - bp.A[1], b.P[2] - bp.A[2]};
         const double QC[3] = {k.P[0] - kp.A[0], k.P[1] - kp.A[1], k.P[2] - kp.A[2]};
-        const double a2 = 2.0 * b.aa, b2 = 2.0 * (b.p - b.aa), c2 = 2.0 * k.aa;
+        const R a2 = R(2.0 * b.aa), b2 = R(2.0 * (b.p - b.aa)), c2 = R(2.0 * k.aa);
+        // FP32 share: this primitive quartet's derivatives in R, then added to the FP64 sums
+        R pA[3] = {0, 0, 0}, pB[3] = {0, 0, 0}, pC[3] = {0, 0, 0};
 #pragma unroll
         for (int r = 0; r < NR; ++r) {
           const double t2 = rt[r];
@@ -507,12 +529,12 @@ __global__ void __launch_bounds__(128, (LA + LB + LC + LD <= 1) ? 4 : 1) grad_ke
           const double b00 = 0.5 * t2 * inv_s, h = 0.5 - 0.5 * t2;
           const double b10 = fma(h, b.inv_p, b00), b01 = fma(h, k.inv_p, b00);
           const double f2 = t2 * q * inv_s, f3 = t2 * p * inv_s;
-          double E[3][ESZ];
+          R E[3][ESZ];
 #pragma unroll
           for (int ax = 0; ax < 3; ++ax)
-            axis_table<double, LA + LB + 1, LC + LD + 1, EA, EB, EC, ED>(
-                PA[ax] - f2 * PQ[ax], QC[ax] + f3 * PQ[ax], b00, b10, b01, AB[ax], CD[ax],
-                ax == 2 ? wt[r] * pref : 1.0, E[ax]);
+            axis_table<R, LA + LB + 1, LC + LD + 1, EA, EB, EC, ED>(
+                R(PA[ax] - f2 * PQ[ax]), R(QC[ax] + f3 * PQ[ax]), R(b00), R(b10), R(b01), R(AB[ax]), R(CD[ax]),
+                R(ax == 2 ? wt[r] * pref : 1.0), E[ax]);
 #pragma unroll
           for (int a = 0; a < C::NA; ++a)
 #pragma unroll
@@ -521,25 +543,39 @@ __global__ void __launch_bounds__(128, (LA + LB + LC + LD <= 1) ? 4 : 1) grad_ke
               for (int c = 0; c < C::NC; ++c)
 #pragma unroll
                 for (int d = 0; d < C::ND; ++d) {
-                  const double w = W[((a * C::NB + bb) * C::NC + c) * C::ND + d];
-                  double reg[3], dA[3], dB[3], dC[3];
+                  const R w = W[((a * C::NB + bb) * C::NC + c) * C::ND + d];
+                  R reg[3], dA[3], dB[3], dC[3];
 #pragma unroll
                   for (int ax = 0; ax < 3; ++ax) {
                     const int ia = cart_pow(LA, a, ax), ib = cart_pow(LB, bb, ax), ic = cart_pow(LC, c, ax),
                               id = cart_pow(LD, d, ax);
                     reg[ax] = E[ax][eidx(ia, ib, ic, id)];
                     dA[ax] = a2 * E[ax][eidx(ia + 1, ib, ic, id)] -
-                             (ia > 0 ? double(ia) * E[ax][eidx(ia > 0 ? ia - 1 : 0, ib, ic, id)] : 0.0);
+                             (ia > 0 ? R(ia) * E[ax][eidx(ia > 0 ? ia - 1 : 0, ib, ic, id)] : R(0));
                     dB[ax] = b2 * E[ax][eidx(ia, ib + 1, ic, id)] -
-                             (ib > 0 ? double(ib) * E[ax][eidx(ia, ib > 0 ? ib - 1 : 0, ic, id)] : 0.0);
+                             (ib > 0 ? R(ib) * E[ax][eidx(ia, ib > 0 ? ib - 1 : 0, ic, id)] : R(0));
                     dC[ax] = c2 * E[ax][eidx(ia, ib, ic + 1, id)] -
-                             (ic > 0 ? double(ic) * E[ax][eidx(ia, ib, ic > 0 ? ic - 1 : 0, id)] : 0.0);
+                             (ic > 0 ? R(ic) * E[ax][eidx(ia, ib, ic > 0 ? ic - 1 : 0, id)] : R(0));
                   }
-                  const double wyz = w * reg[1] * reg[2], wxz = w * reg[0] * reg[2], wxy = w * reg[0] * reg[1];
-                  gAq[0] = fma(wyz, dA[0], gAq[0]); gAq[1] = fma(wxz, dA[1], gAq[1]); gAq[2] = fma(wxy, dA[2], gAq[2]);
-                  gBq[0] = fma(wyz, dB[0], gBq[0]); gBq[1] = fma(wxz, dB[1], gBq[1]); gBq[2] = fma(wxy, dB[2], gBq[2]);
-                  gC[0] = fma(wyz, dC[0], gC[0]); gC[1] = fma(wxz, dC[1], gC[1]); gC[2] = fma(wxy, dC[2], gC[2]);
+                  const R wyz = w * reg[1] * reg[2], wxz = w * reg[0] * reg[2], wxy = w * reg[0] * reg[1];
+                  if constexpr (F32) {
+                    pA[0] = fmaf(wyz, dA[0], pA[0]); pA[1] = fmaf(wxz, dA[1], pA[1]); pA[2] = fmaf(wxy, dA[2], pA[2]);
+                    pB[0] = fmaf(wyz, dB[0], pB[0]); pB[1] = fmaf(wxz, dB[1], pB[1]); pB[2] = fmaf(wxy, dB[2], pB[2]);
+                    pC[0] = fmaf(wyz, dC[0], pC[0]); pC[1] = fmaf(wxz, dC[1], pC[1]); pC[2] = fmaf(wxy, dC[2], pC[2]);
+                  } else {
+                    gAq[0] = fma(wyz, dA[0], gAq[0]); gAq[1] = fma(wxz, dA[1], gAq[1]); gAq[2] = fma(wxy, dA[2], gAq[2]);
+                    gBq[0] = fma(wyz, dB[0], gBq[0]); gBq[1] = fma(wxz, dB[1], gBq[1]); gBq[2] = fma(wxy, dB[2], gBq[2]);
+                    gC[0] = fma(wyz, dC[0], gC[0]); gC[1] = fma(wxz, dC[1], gC[1]); gC[2] = fma(wxy, dC[2], gC[2]);
+                  }
                 }
+        }
+        if constexpr (F32) {
+#pragma unroll
+          for (int x = 0; x < 3; ++x) {
+            gAq[x] += double(pA[x]);
+            gBq[x] += double(pB[x]);
+            gC[x] += double(pC[x]);
+          }
         }
       }
     }

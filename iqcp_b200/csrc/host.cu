@@ -28,6 +28,8 @@ struct TaskRange {
   int first, count;         // into the task array
   long long quartets;       // screened shell quartets in the range
   int mode[2];              // kernel variant for J/K [0] and gradient [1]
+  int mode32[2];            // the same for the FP32 share of a mixed call
+  int split[2];             // mixed form: 1 = FP64 + FP32 passes, 0 = the whole class in FP64
 };
 
 }  // namespace
@@ -62,14 +64,22 @@ struct iqcp_ctx {
   double* d_Kt = nullptr;
   double* d_io[4] = {nullptr, nullptr, nullptr, nullptr};  // staging for host-buffer calls
   double* d_grad = nullptr;
-  // mixed precision: per shell-pair max |D| and the FP32 quartet counter
+  // mixed precision: per shell-block max |D| of every molecule (ns_m x ns_m
+  // at d_dbase[m]), the FP32 quartet counter and the per-task FP32 masks
   double* d_dmax = nullptr;
+  long long* d_dbase = nullptr;
+  int* d_mol_shell0 = nullptr;
+  int* d_mol_ns = nullptr;
+  long long dmax_total = 0;
   unsigned long long* d_fp32 = nullptr;
-  int* d_counters = nullptr;      // one work counter per class range and kind
+  unsigned* d_mask = nullptr;
+  int n_tasks = 0;
+  int* d_counters = nullptr;      // one work counter per class range, kind and pass
   int* cur_counter = nullptr;
   bool mixed_call = false;
+  bool in_capture = false;        // the last call was enqueued into a CUDA graph capture
   // basis copy for the one-electron kernel
-  int* d_bint = nullptr;          // l | nprim | pstart | off | z
+  int* d_bint = nullptr;          // l | nprim | pstart | off | z | atom (per shell, molecule-local)
   double* d_bdbl = nullptr;       // center | exps | coefs | atom_xyz
   int n_prims = 0;
   // host copies
@@ -83,7 +93,8 @@ struct iqcp_ctx {
   // per-launch timing of the quartet kernels (off unless requested)
   bool profile = false;
   std::vector<cudaEvent_t> pev;
-  struct LaunchRec { int kind, X, Y; float ms; long long quartets; };
+  // kind: 0 J/K, 1 gradient, 2 / 3 their FP32 share in a mixed call
+  struct LaunchRec { int kind, X, Y; float ms; long long quartets; int ev; };
   std::vector<LaunchRec> launch_log;
   int launches_total = 0;       // every kernel of the last call
   // surviving primitive quartets per task range (counted on first request)
@@ -172,7 +183,8 @@ void build_tasks(iqcp_ctx* ctx, std::vector<int>& ket_list, std::vector<QuartetT
   ctx->n_quartets = 0;
   for (int X = 0; X < NC; ++X)
     for (int Y = 0; Y <= X; ++Y) {
-      TaskRange r{X, Y, (int)tasks.size(), 0, 0, {default_mode(X, Y, 0), default_mode(X, Y, 1)}};
+      TaskRange r{X, Y, (int)tasks.size(), 0, 0, {default_mode(X, Y, 0), default_mode(X, Y, 1)},
+                  {default_mode(X, Y, 0), default_mode(X, Y, 1)}, {1, 1}};
       for (int m = 0; m < ctx->n_mol; ++m) {
         const size_t lx = (size_t)m * NC + X, ly = (size_t)m * NC + Y;
         const auto& LX = lists[lx];
@@ -214,7 +226,7 @@ int ensure_device(iqcp_ctx* ctx) {
 }
 
 int ensure_profile_events(iqcp_ctx* ctx) {
-  const size_t need = 2 * ctx->ranges.size();
+  const size_t need = 4 * ctx->ranges.size();
   while (ctx->pev.size() < need) {
     cudaEvent_t e;
     CK(cudaEventCreate(&e));
@@ -223,30 +235,119 @@ int ensure_profile_events(iqcp_ctx* ctx) {
   return IQCP_OK;
 }
 
-// Launch one quartet kernel per non-empty class range; kind 0 = J/K, 1 = gradient.
+Mixed mixed_args(const iqcp_ctx* ctx, int pass) {
+  Mixed m;
+  m.dmax = ctx->d_dmax;
+  m.dbase = ctx->d_dbase;
+  m.shell0 = ctx->d_mol_shell0;
+  m.ns = ctx->d_mol_ns;
+  m.cutoff = ctx->opt.mixed_cutoff;
+  m.pass = pass;
+  m.fp32_count = pass == 2 ? ctx->d_fp32 : nullptr;
+  m.mask = ctx->d_mask;
+  return m;
+}
+
+JKArgs jk_args(const iqcp_ctx* ctx, const TaskRange& r, const double* Ds, double* Jt, double* Kt, int mode,
+               int pass, int* counter) {
+  JKArgs a;
+  a.pairs = ctx->d_pairs;
+  a.pp = ctx->d_pp;
+  a.ket_list = ctx->d_ket_list;
+  a.tasks = ctx->d_tasks + r.first;
+  a.ntasks = r.count;
+  a.D = Ds;
+  a.nbf = ctx->nbf;
+  a.J = Jt;
+  a.K = Kt;
+  a.prim_thr = ctx->opt.prim_threshold;
+  a.mode = mode;
+  a.mx = mixed_args(ctx, pass);
+  a.mx.mask = ctx->d_mask + r.first;
+  a.next_task = counter;
+  a.mol_base = ctx->d_mol_base;
+  a.mol_n = ctx->d_mol_n;
+  return a;
+}
+
+GradArgs grad_args(const iqcp_ctx* ctx, const TaskRange& r, const double* Ds, double xscale, double* grad,
+                   int mode, int pass, int* counter) {
+  GradArgs a;
+  a.pairs = ctx->d_pairs;
+  a.pp = ctx->d_pp;
+  a.ket_list = ctx->d_ket_list;
+  a.tasks = ctx->d_tasks + r.first;
+  a.ntasks = r.count;
+  a.D = Ds;
+  a.nbf = ctx->nbf;
+  a.xscale = xscale;
+  a.grad = grad;
+  a.prim_thr = ctx->opt.prim_threshold;
+  a.schwarz_thr = ctx->opt.schwarz_threshold;
+  a.natoms = ctx->n_atoms;
+  a.gsmem = ctx->n_atoms <= 2048 ? 1 : 0;
+  a.mode = mode;
+  a.mx = mixed_args(ctx, pass);
+  a.mx.mask = ctx->d_mask + r.first;
+  a.next_task = counter;
+  a.mol_base = ctx->d_mol_base;
+  a.mol_n = ctx->d_mol_n;
+  return a;
+}
+
+// Mixed form for density dD (unscaled): per-shell-block density bound, then
+// the FP32 mask of every task (kind 0 J/K, 1 gradient)
+int prepare_mixed(iqcp_ctx* ctx, const double* dD, int kind) {
+  CK(launch_shell_dmax(dD, ctx->pack, ctx->d_bint + 3 * ctx->n_shells, ctx->d_bint, mixed_args(ctx, 0),
+                       ctx->dmax_total, ctx->d_dmax, ctx->stream));
+  CK(launch_precision_masks(ctx->d_pairs, ctx->d_ket_list, ctx->d_tasks, ctx->n_tasks, mixed_args(ctx, 1),
+                            kind == 1, ctx->d_mask, ctx->stream));
+  CK(cudaMemsetAsync(ctx->d_fp32, 0, sizeof(unsigned long long), ctx->stream));
+  ctx->launches_total += 2;
+  return IQCP_OK;
+}
+
+// True while the context stream is being captured into a CUDA graph: the
+// device entry points then only enqueue work (no timing events, no stats read
+// back, no host synchronisation).
+bool capturing(const iqcp_ctx* ctx) {
+  cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(ctx->stream, &st) != cudaSuccess) return false;
+  return st != cudaStreamCaptureStatusNone;
+}
+
+// Launch the quartet kernels of every non-empty class range; kind 0 = J/K,
+// 1 = gradient.  In a mixed call a class whose split flag is set launches
+// twice, pass 1 (FP64 share) then pass 2 (FP32 share); launch(r, pass,
+// counter) issues one launch.
 template <typename F>
 int run_ranges(iqcp_ctx* ctx, int kind, F&& launch) {
-  // launch(r) reads ctx->cur_counter for the range's work counter
-  if (ctx->profile) {
+  ctx->in_capture = capturing(ctx);
+  const bool prof = ctx->profile && !ctx->in_capture;
+  if (prof) {
     int rc = ensure_profile_events(ctx);
     if (rc) return rc;
   }
+  const size_t nr = ctx->ranges.size();
   ctx->launch_log.clear();
-  CK(cudaMemsetAsync(ctx->d_counters + kind * ctx->ranges.size(), 0, sizeof(int) * ctx->ranges.size(),
-                     ctx->stream));
-  CK(cudaEventRecord(ctx->ev0, ctx->stream));
+  CK(cudaMemsetAsync(ctx->d_counters + 2 * kind * nr, 0, sizeof(int) * 2 * nr, ctx->stream));
+  if (!ctx->in_capture) CK(cudaEventRecord(ctx->ev0, ctx->stream));
   int launches = 0;
-  for (size_t i = 0; i < ctx->ranges.size(); ++i) {
+  for (size_t i = 0; i < nr; ++i) {
     const TaskRange& r = ctx->ranges[i];
     if (r.count == 0) continue;
-    if (ctx->profile) CK(cudaEventRecord(ctx->pev[2 * i], ctx->stream));
-    ctx->cur_counter = ctx->d_counters + kind * ctx->ranges.size() + i;
-    CK(launch(r));
-    if (ctx->profile) CK(cudaEventRecord(ctx->pev[2 * i + 1], ctx->stream));
-    ++launches;
-    ctx->launch_log.push_back({kind, r.X, r.Y, 0.f, r.quartets});
+    const bool split = ctx->mixed_call && r.split[kind];
+    for (int ps = 0; ps < (split ? 2 : 1); ++ps) {
+      const int pass = split ? ps + 1 : 0;
+      const int ev = int(2 * (2 * i + ps));
+      if (prof) CK(cudaEventRecord(ctx->pev[ev], ctx->stream));
+      CK(launch(r, pass, ctx->d_counters + (2 * kind + ps) * nr + i));
+      if (prof) CK(cudaEventRecord(ctx->pev[ev + 1], ctx->stream));
+      ++launches;
+      ctx->launch_log.push_back({kind + (pass == 2 ? 2 : 0), r.X, r.Y, 0.f, pass == 2 ? 0 : r.quartets, ev});
+    }
   }
-  CK(cudaEventRecord(ctx->ev1, ctx->stream));
+  if (!ctx->in_capture) CK(cudaEventRecord(ctx->ev1, ctx->stream));
   ctx->stats[0] = (double)ctx->n_quartets;
   ctx->stats[1] = launches;
   ctx->launches_total += launches;
@@ -254,45 +355,25 @@ int run_ranges(iqcp_ctx* ctx, int kind, F&& launch) {
 }
 
 int run_jk_device(iqcp_ctx* ctx, const double* dD, bool want_k) {
-  const int n = ctx->nbf;
   const size_t bytes = sizeof(double) * (size_t)ctx->packed;
   ctx->launches_total = 1;
   CK(launch_scale_density(dD, ctx->d_ang, ctx->pack, ctx->d_Ds, ctx->stream));
-  // the mixed form's per-shell-pair |D| bound is kept for single geometries
-  ctx->mixed_call = ctx->opt.precision == IQCP_MIXED && ctx->n_mol == 1;
+  ctx->mixed_call = ctx->opt.precision == IQCP_MIXED;
   if (ctx->mixed_call) {
-    CK(launch_shell_dmax(dD, ctx->d_bint + 3 * ctx->n_shells, ctx->d_bint, ctx->n_shells, n, ctx->d_dmax,
-                         ctx->stream));
-    CK(cudaMemsetAsync(ctx->d_fp32, 0, sizeof(unsigned long long), ctx->stream));
-    ctx->launches_total += 1;
+    int rc = prepare_mixed(ctx, dD, 0);
+    if (rc) return rc;
   }
   CK(cudaMemsetAsync(ctx->d_Jt, 0, bytes, ctx->stream));
   if (want_k) CK(cudaMemsetAsync(ctx->d_Kt, 0, bytes, ctx->stream));
-  return run_ranges(ctx, 0, [&](const TaskRange& r) {
-    JKArgs a;
-    a.pairs = ctx->d_pairs;
-    a.pp = ctx->d_pp;
-    a.ket_list = ctx->d_ket_list;
-    a.tasks = ctx->d_tasks + r.first;
-    a.ntasks = r.count;
-    a.D = ctx->d_Ds;
-    a.nbf = n;
-    a.J = ctx->d_Jt;
-    a.K = want_k ? ctx->d_Kt : nullptr;
-    a.prim_thr = ctx->opt.prim_threshold;
-    a.mode = r.mode[0];
-    a.dmax_shell = ctx->mixed_call ? ctx->d_dmax : nullptr;
-    a.n_shells = ctx->n_shells;
-    a.mixed_cutoff = ctx->opt.mixed_cutoff;
-    a.fp32_count = ctx->mixed_call ? ctx->d_fp32 : nullptr;
-    a.next_task = ctx->cur_counter;
-    a.mol_base = ctx->d_mol_base;
-    a.mol_n = ctx->d_mol_n;
+  return run_ranges(ctx, 0, [&](const TaskRange& r, int pass, int* counter) {
+    const JKArgs a = jk_args(ctx, r, ctx->d_Ds, ctx->d_Jt, want_k ? ctx->d_Kt : nullptr,
+                             pass == 2 ? r.mode32[0] : r.mode[0], pass, counter);
     return launch_jk(r.X, r.Y, a, ctx->stream);
   });
 }
 
 int finish_stats(iqcp_ctx* ctx) {
+  if (ctx->in_capture) return IQCP_OK;
   float ms = 0.f;
   CK(cudaEventSynchronize(ctx->ev1));
   CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
@@ -305,12 +386,10 @@ int finish_stats(iqcp_ctx* ctx) {
     ctx->stats[3] = (double)c;
   }
   if (ctx->profile) {
-    size_t k = 0;
-    for (size_t i = 0; i < ctx->ranges.size(); ++i) {
-      if (ctx->ranges[i].count == 0) continue;
+    for (auto& rec : ctx->launch_log) {
       float t = 0.f;
-      CK(cudaEventElapsedTime(&t, ctx->pev[2 * i], ctx->pev[2 * i + 1]));
-      ctx->launch_log[k++].ms = t;
+      CK(cudaEventElapsedTime(&t, ctx->pev[rec.ev], ctx->pev[rec.ev + 1]));
+      rec.ms = t;
     }
   }
   return IQCP_OK;
@@ -389,7 +468,7 @@ static int create_batch(int nmol, const iqcp_basis_desc* descs, const iqcp_optio
 
   // concatenate the molecules: global shell, atom, primitive and basis-function
   // numbering; basis offsets inside a pair stay local to its molecule block
-  std::vector<int> bl, bnp, bps, boff, bz;
+  std::vector<int> bl, bnp, bps, boff, bz, bat;
   std::vector<double> bc, bex, bco, bxyz, ang;
   std::vector<PrimPair> pps;
   long long base = 0;
@@ -413,6 +492,7 @@ static int create_batch(int nmol, const iqcp_basis_desc* descs, const iqcp_optio
       ctx->shell_atom.push_back(a0 + b->atom_of_shell[s]);
       for (int c = 0; c < ncart(b->l[s]); ++c) ang.push_back(ang_host(b->l[s], c));
       bl.push_back(b->l[s]);
+      bat.push_back(b->atom_of_shell[s]);
       bnp.push_back(b->nprim[s]);
       bps.push_back(p0 + pstart[s]);
       boff.push_back(off);
@@ -488,6 +568,7 @@ static int create_batch(int nmol, const iqcp_basis_desc* descs, const iqcp_optio
     bi.insert(bi.end(), bps.begin(), bps.end());
     bi.insert(bi.end(), boff.begin(), boff.end());
     bi.insert(bi.end(), bz.begin(), bz.end());
+    bi.insert(bi.end(), bat.begin(), bat.end());
     std::vector<double> bd;
     bd.insert(bd.end(), bc.begin(), bc.end());
     bd.insert(bd.end(), bex.begin(), bex.end());
@@ -538,6 +619,8 @@ static int create_batch(int nmol, const iqcp_basis_desc* descs, const iqcp_optio
   build_tasks(ctx, ket_list, tasks);
   if (ket_list.empty()) ket_list.push_back(0);
   if (tasks.empty()) tasks.push_back(QuartetTask());
+  ctx->n_tasks = (int)tasks.size();
+  CK(cudaMalloc(&ctx->d_mask, sizeof(unsigned) * tasks.size()));
   CK(cudaMalloc(&ctx->d_ket_list, sizeof(int) * ket_list.size()));
   CK(cudaMemcpy(ctx->d_ket_list, ket_list.data(), sizeof(int) * ket_list.size(), cudaMemcpyHostToDevice));
   CK(cudaMalloc(&ctx->d_tasks, sizeof(QuartetTask) * tasks.size()));
@@ -551,8 +634,23 @@ static int create_batch(int nmol, const iqcp_basis_desc* descs, const iqcp_optio
   CK(cudaMalloc(&ctx->d_Kt, sizeof(double) * nn));
   for (int i = 0; i < 4; ++i) CK(cudaMalloc(&ctx->d_io[i], sizeof(double) * nn));
   CK(cudaMalloc(&ctx->d_grad, sizeof(double) * 3 * ctx->n_atoms));
-  if (nmol == 1) CK(cudaMalloc(&ctx->d_dmax, sizeof(double) * (size_t)ctx->n_shells * ctx->n_shells));
-  CK(cudaMalloc(&ctx->d_counters, sizeof(int) * 2 * (ctx->ranges.size() + 1)));
+  {
+    std::vector<long long> dbase(nmol + 1, 0);
+    std::vector<int> ns(nmol);
+    for (int m = 0; m < nmol; ++m) {
+      ns[m] = ctx->mol_shell0[m + 1] - ctx->mol_shell0[m];
+      dbase[m + 1] = dbase[m] + (long long)ns[m] * ns[m];
+    }
+    ctx->dmax_total = dbase[nmol];
+    CK(cudaMalloc(&ctx->d_dmax, sizeof(double) * ctx->dmax_total));
+    CK(cudaMalloc(&ctx->d_dbase, sizeof(long long) * (nmol + 1)));
+    CK(cudaMalloc(&ctx->d_mol_shell0, sizeof(int) * nmol));
+    CK(cudaMalloc(&ctx->d_mol_ns, sizeof(int) * nmol));
+    CK(cudaMemcpy(ctx->d_dbase, dbase.data(), sizeof(long long) * (nmol + 1), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->d_mol_shell0, ctx->mol_shell0.data(), sizeof(int) * nmol, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->d_mol_ns, ns.data(), sizeof(int) * nmol, cudaMemcpyHostToDevice));
+  }
+  CK(cudaMalloc(&ctx->d_counters, sizeof(int) * 4 * (ctx->ranges.size() + 1)));
   CK(cudaMalloc(&ctx->d_fp32, sizeof(unsigned long long)));
   return IQCP_OK;
 }
@@ -593,6 +691,10 @@ void iqcp_destroy(iqcp_ctx* ctx) {
   cudaFree(ctx->d_bint);
   cudaFree(ctx->d_bdbl);
   cudaFree(ctx->d_dmax);
+  cudaFree(ctx->d_dbase);
+  cudaFree(ctx->d_mol_shell0);
+  cudaFree(ctx->d_mol_ns);
+  cudaFree(ctx->d_mask);
   cudaFree(ctx->d_mol_base);
   cudaFree(ctx->d_mol_n);
   cudaFree(ctx->d_mol_bf0);
@@ -703,26 +805,8 @@ int iqcp_jk_device_noalloc(iqcp_ctx* ctx, const double* dD, double* dJ, double* 
   CK(launch_scale_density(dD, ctx->d_ang, ctx->pack, Ds, ctx->stream));
   CK(cudaMemsetAsync(Jt, 0, sizeof(double) * nn, ctx->stream));
   if (want_k) CK(cudaMemsetAsync(Kt, 0, sizeof(double) * nn, ctx->stream));
-  rc = run_ranges(ctx, 0, [&](const TaskRange& r) {
-    JKArgs a;
-    a.pairs = ctx->d_pairs;
-    a.pp = ctx->d_pp;
-    a.ket_list = ctx->d_ket_list;
-    a.tasks = ctx->d_tasks + r.first;
-    a.ntasks = r.count;
-    a.D = Ds;
-    a.nbf = n;
-    a.J = Jt;
-    a.K = want_k ? Kt : nullptr;
-    a.prim_thr = ctx->opt.prim_threshold;
-    a.mode = r.mode[0];
-    a.dmax_shell = nullptr;  // FP64 only
-    a.n_shells = ctx->n_shells;
-    a.mixed_cutoff = 0.0;
-    a.fp32_count = nullptr;
-    a.next_task = ctx->cur_counter;
-    a.mol_base = ctx->d_mol_base;
-    a.mol_n = ctx->d_mol_n;
+  rc = run_ranges(ctx, 0, [&](const TaskRange& r, int pass, int* counter) {
+    const JKArgs a = jk_args(ctx, r, Ds, Jt, want_k ? Kt : nullptr, r.mode[0], pass, counter);  // FP64 only
     return launch_jk(r.X, r.Y, a, ctx->stream);
   });
   ctx->profile = prof;
@@ -772,29 +856,16 @@ int iqcp_eri_grad_device(iqcp_ctx* ctx, const double* dD, double hf_frac, double
   if (!ctx || !dD || !dgrad) return IQCP_ERR_ARG;
   int rc = ensure_device(ctx);
   if (rc) return rc;
-  const int n = ctx->nbf;
   ctx->launches_total = 1;
-  ctx->mixed_call = false;
   CK(launch_scale_density(dD, ctx->d_ang, ctx->pack, ctx->d_Ds, ctx->stream));
-  rc = run_ranges(ctx, 1, [&](const TaskRange& r) {
-    GradArgs a;
-    a.pairs = ctx->d_pairs;
-    a.pp = ctx->d_pp;
-    a.ket_list = ctx->d_ket_list;
-    a.tasks = ctx->d_tasks + r.first;
-    a.ntasks = r.count;
-    a.D = ctx->d_Ds;
-    a.nbf = n;
-    a.xscale = 0.25 * hf_frac;
-    a.grad = dgrad;
-    a.prim_thr = ctx->opt.prim_threshold;
-    a.schwarz_thr = ctx->opt.schwarz_threshold;
-    a.natoms = ctx->n_atoms;
-    a.gsmem = ctx->n_atoms <= 2048 ? 1 : 0;
-    a.mode = r.mode[1];
-    a.next_task = ctx->cur_counter;
-    a.mol_base = ctx->d_mol_base;
-    a.mol_n = ctx->d_mol_n;
+  ctx->mixed_call = ctx->opt.precision == IQCP_MIXED;
+  if (ctx->mixed_call) {
+    rc = prepare_mixed(ctx, dD, 1);
+    if (rc) return rc;
+  }
+  rc = run_ranges(ctx, 1, [&](const TaskRange& r, int pass, int* counter) {
+    const GradArgs a = grad_args(ctx, r, ctx->d_Ds, 0.25 * hf_frac, dgrad, pass == 2 ? r.mode32[1] : r.mode[1],
+                                 pass, counter);
     return launch_grad(r.X, r.Y, a, ctx->stream);
   });
   if (rc) return rc;
@@ -844,29 +915,36 @@ int iqcp_eri_compressed(iqcp_ctx* ctx, double* out, long long out_len) {
   return IQCP_OK;
 }
 
+static OneEArgs one_e_args(const iqcp_ctx* ctx, int m) {
+  const int ns = ctx->n_shells;
+  const int s0 = ctx->mol_shell0[m], a0 = ctx->mol_atom0[m];
+  OneEArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.n_shells = ctx->mol_shell0[m + 1] - s0;
+  a.n_atoms = ctx->mol_atom0[m + 1] - a0;
+  a.nbf = ctx->mol_nbf[m];
+  a.l = ctx->d_bint + s0;
+  a.nprim = ctx->d_bint + ns + s0;
+  a.pstart = ctx->d_bint + 2 * ns + s0;
+  a.off = ctx->d_bint + 3 * ns + s0;
+  a.z = ctx->d_bint + 4 * ns + a0;
+  a.atom = ctx->d_bint + 4 * ns + ctx->n_atoms + s0;
+  a.center = ctx->d_bdbl + 3 * s0;
+  a.exps = ctx->d_bdbl + 3 * ns;
+  a.coefs = a.exps + ctx->n_prims;
+  a.atom_xyz = a.coefs + ctx->n_prims + 3 * a0;
+  return a;
+}
+
 int iqcp_one_electron(iqcp_ctx* ctx, double* S, double* T, double* V) {
   if (!ctx) return IQCP_ERR_ARG;
   int rc = ensure_device(ctx);
   if (rc) return rc;
-  const int ns = ctx->n_shells;
   const size_t bytes = sizeof(double) * (size_t)ctx->packed;
   // one launch per molecule block of the packed matrices
   for (int m = 0; m < ctx->n_mol; ++m) {
-    const int s0 = ctx->mol_shell0[m], a0 = ctx->mol_atom0[m];
     const long long mb = ctx->mol_base[m];
-    OneEArgs a;
-    a.n_shells = ctx->mol_shell0[m + 1] - s0;
-    a.n_atoms = ctx->mol_atom0[m + 1] - a0;
-    a.nbf = ctx->mol_nbf[m];
-    a.l = ctx->d_bint + s0;
-    a.nprim = ctx->d_bint + ns + s0;
-    a.pstart = ctx->d_bint + 2 * ns + s0;
-    a.off = ctx->d_bint + 3 * ns + s0;
-    a.z = ctx->d_bint + 4 * ns + a0;
-    a.center = ctx->d_bdbl + 3 * s0;
-    a.exps = ctx->d_bdbl + 3 * ns;
-    a.coefs = a.exps + ctx->n_prims;
-    a.atom_xyz = a.coefs + ctx->n_prims + 3 * a0;
+    OneEArgs a = one_e_args(ctx, m);
     a.S = S ? ctx->d_io[0] + mb : nullptr;
     a.T = T ? ctx->d_io[1] + mb : nullptr;
     a.V = V ? ctx->d_io[2] + mb : nullptr;
@@ -875,6 +953,56 @@ int iqcp_one_electron(iqcp_ctx* ctx, double* S, double* T, double* V) {
   if (S) CK(cudaMemcpyAsync(S, ctx->d_io[0], bytes, cudaMemcpyDeviceToHost, ctx->stream));
   if (T) CK(cudaMemcpyAsync(T, ctx->d_io[1], bytes, cudaMemcpyDeviceToHost, ctx->stream));
   if (V) CK(cudaMemcpyAsync(V, ctx->d_io[2], bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return IQCP_OK;
+}
+
+int iqcp_one_electron_grad_device(iqcp_ctx* ctx, const double* dD, const double* dW, double* dgrad) {
+  if (!ctx || !dD || !dW || !dgrad) return IQCP_ERR_ARG;
+  int rc = ensure_device(ctx);
+  if (rc) return rc;
+  for (int m = 0; m < ctx->n_mol; ++m) {
+    const long long mb = ctx->mol_base[m];
+    OneEArgs a = one_e_args(ctx, m);
+    a.D = dD + mb;
+    a.W = dW + mb;
+    a.grad = dgrad + 3 * ctx->mol_atom0[m];
+    a.gsmem = a.n_atoms <= 2048 ? 1 : 0;
+    CK(launch_one_electron_grad(a, ctx->stream));
+  }
+  return IQCP_OK;
+}
+
+int iqcp_one_electron_grad(iqcp_ctx* ctx, const double* D, const double* W, double* grad) {
+  if (!ctx || !D || !W || !grad) return IQCP_ERR_ARG;
+  int rc = ensure_device(ctx);
+  if (rc) return rc;
+  const size_t bytes = sizeof(double) * (size_t)ctx->packed;
+  const size_t gb = sizeof(double) * 3 * ctx->n_atoms;
+  CK(cudaMemcpyAsync(ctx->d_io[0], D, bytes, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->d_io[1], W, bytes, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->d_grad, grad, gb, cudaMemcpyHostToDevice, ctx->stream));
+  rc = iqcp_one_electron_grad_device(ctx, ctx->d_io[0], ctx->d_io[1], ctx->d_grad);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(grad, ctx->d_grad, gb, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return IQCP_OK;
+}
+
+int iqcp_rhf_gradient(iqcp_ctx* ctx, const double* D, const double* W, double* grad) {
+  if (!ctx || !D || !W || !grad) return IQCP_ERR_ARG;
+  int rc = ensure_device(ctx);
+  if (rc) return rc;
+  const size_t bytes = sizeof(double) * (size_t)ctx->packed;
+  const size_t gb = sizeof(double) * 3 * ctx->n_atoms;
+  CK(cudaMemcpyAsync(ctx->d_io[0], D, bytes, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->d_io[1], W, bytes, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemsetAsync(ctx->d_grad, 0, gb, ctx->stream));
+  rc = iqcp_one_electron_grad_device(ctx, ctx->d_io[0], ctx->d_io[1], ctx->d_grad);
+  if (rc) return rc;
+  rc = iqcp_eri_grad_device(ctx, ctx->d_io[0], 1.0, ctx->d_grad);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(grad, ctx->d_grad, gb, cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
   return IQCP_OK;
 }
@@ -920,65 +1048,73 @@ int iqcp_kernel_launches(const iqcp_ctx* ctx) { return ctx ? ctx->launches_total
 
 // Autotuner: time every class range with every kernel variant on this
 // density (best of `reps` runs each) and keep the fastest variant per class
-// and per kind (J/K, gradient).  Results are the same up to rounding whichever
-// variant runs; only the speed differs.
+// and per kind (J/K, gradient).  In the mixed form the FP64 and FP32 shares
+// are tuned separately at the current cutoff, and a class is split into the
+// two passes only where that beats running it wholly in FP64.  Results are
+// the same up to rounding whichever variant runs; only the speed differs.
 int iqcp_autotune(iqcp_ctx* ctx, const double* dD, int reps) {
   if (!ctx || !dD) return IQCP_ERR_ARG;
   int rc = ensure_device(ctx);
   if (rc) return rc;
   if (reps < 1) reps = 1;
-  const int n = ctx->nbf;
   const size_t bytes = sizeof(double) * (size_t)ctx->packed;
   CK(launch_scale_density(dD, ctx->d_ang, ctx->pack, ctx->d_Ds, ctx->stream));
+  const bool mixed = ctx->opt.precision == IQCP_MIXED;
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
+  // best time over the variants of one (range, kind, pass); mode_out gets the winner
+  auto tune = [&](TaskRange& r, int kind, int pass, int* mode_out, float* t_out) -> int {
+    float best = 1e30f;
+    for (int mode = 0; mode < kNumModes; ++mode) {
+      if (pass == 2 && mode == 3) continue;  // the FP32 share has no 32-lane variant
+      float tmin = 1e30f;
+      for (int rep = 0; rep < reps + 1; ++rep) {  // first run warms caches and sets attributes
+        CK(cudaMemsetAsync(ctx->d_Jt, 0, bytes, ctx->stream));
+        CK(cudaMemsetAsync(ctx->d_Kt, 0, bytes, ctx->stream));
+        CK(cudaMemsetAsync(ctx->d_grad, 0, sizeof(double) * 3 * ctx->n_atoms, ctx->stream));
+        CK(cudaMemsetAsync(ctx->d_counters, 0, sizeof(int), ctx->stream));
+        CK(cudaEventRecord(e0, ctx->stream));
+        if (kind == 0) {
+          const JKArgs a = jk_args(ctx, r, ctx->d_Ds, ctx->d_Jt, ctx->d_Kt, mode, pass, ctx->d_counters);
+          CK(launch_jk(r.X, r.Y, a, ctx->stream));
+        } else {
+          const GradArgs a = grad_args(ctx, r, ctx->d_Ds, 0.25, ctx->d_grad, mode, pass, ctx->d_counters);
+          CK(launch_grad(r.X, r.Y, a, ctx->stream));
+        }
+        CK(cudaEventRecord(e1, ctx->stream));
+        CK(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, e0, e1));
+        if (rep > 0) tmin = std::min(tmin, ms);
+      }
+      if (tmin < best) {
+        best = tmin;
+        *mode_out = mode;
+      }
+    }
+    *t_out = best;
+    return IQCP_OK;
+  };
   for (int kind = 0; kind < 2; ++kind) {
+    if (mixed) {
+      rc = prepare_mixed(ctx, dD, kind);
+      if (rc) return rc;
+    }
     for (TaskRange& r : ctx->ranges) {
       if (r.count == 0) continue;
-      float best = 1e30f;
-      int best_mode = r.mode[kind];
-      for (int mode = 0; mode < kNumModes; ++mode) {
-        float tmin = 1e30f;
-        for (int rep = 0; rep < reps + 1; ++rep) {  // first run warms caches and sets attributes
-          CK(cudaMemsetAsync(ctx->d_Jt, 0, bytes, ctx->stream));
-          CK(cudaMemsetAsync(ctx->d_Kt, 0, bytes, ctx->stream));
-          CK(cudaMemsetAsync(ctx->d_grad, 0, sizeof(double) * 3 * ctx->n_atoms, ctx->stream));
-          CK(cudaMemsetAsync(ctx->d_counters, 0, sizeof(int), ctx->stream));
-          CK(cudaEventRecord(e0, ctx->stream));
-          if (kind == 0) {
-            JKArgs a;
-            a.pairs = ctx->d_pairs; a.pp = ctx->d_pp; a.ket_list = ctx->d_ket_list;
-            a.tasks = ctx->d_tasks + r.first; a.ntasks = r.count; a.D = ctx->d_Ds; a.nbf = n;
-            a.J = ctx->d_Jt; a.K = ctx->d_Kt; a.prim_thr = ctx->opt.prim_threshold; a.mode = mode;
-            a.dmax_shell = nullptr; a.n_shells = ctx->n_shells; a.mixed_cutoff = 0.0; a.fp32_count = nullptr;
-            a.next_task = ctx->d_counters;
-            a.mol_base = ctx->d_mol_base; a.mol_n = ctx->d_mol_n;
-            CK(launch_jk(r.X, r.Y, a, ctx->stream));
-          } else {
-            GradArgs a;
-            a.pairs = ctx->d_pairs; a.pp = ctx->d_pp; a.ket_list = ctx->d_ket_list;
-            a.tasks = ctx->d_tasks + r.first; a.ntasks = r.count; a.D = ctx->d_Ds; a.nbf = n;
-            a.xscale = 0.25; a.grad = ctx->d_grad; a.prim_thr = ctx->opt.prim_threshold;
-            a.schwarz_thr = ctx->opt.schwarz_threshold;
-    a.natoms = ctx->n_atoms;
-    a.gsmem = ctx->n_atoms <= 2048 ? 1 : 0; a.mode = mode;
-            a.next_task = ctx->d_counters;
-            a.mol_base = ctx->d_mol_base; a.mol_n = ctx->d_mol_n;
-            CK(launch_grad(r.X, r.Y, a, ctx->stream));
-          }
-          CK(cudaEventRecord(e1, ctx->stream));
-          CK(cudaEventSynchronize(e1));
-          float ms = 0.f;
-          CK(cudaEventElapsedTime(&ms, e0, e1));
-          if (rep > 0) tmin = std::min(tmin, ms);
-        }
-        if (tmin < best) {
-          best = tmin;
-          best_mode = mode;
-        }
-      }
-      r.mode[kind] = best_mode;
+      int m0 = r.mode[kind];
+      float t0 = 0.f;
+      if ((rc = tune(r, kind, 0, &m0, &t0))) return rc;
+      r.mode[kind] = m0;
+      if (!mixed) continue;
+      int m1 = m0, m2 = r.mode32[kind];
+      float t1 = 0.f, t2 = 0.f;
+      if ((rc = tune(r, kind, 1, &m1, &t1))) return rc;
+      if ((rc = tune(r, kind, 2, &m2, &t2))) return rc;
+      r.mode32[kind] = m2;
+      r.split[kind] = (t1 + t2 < t0) ? 1 : 0;
+      if (r.split[kind]) r.mode[kind] = m1;
     }
   }
   cudaEventDestroy(e0);
@@ -989,18 +1125,29 @@ int iqcp_autotune(iqcp_ctx* ctx, const double* dD, int reps) {
 // Current kernel variant per (kind, bra class, ket class): modes[2*6*6], -1 when no work.
 int iqcp_kernel_modes(const iqcp_ctx* ctx, int* modes) {
   if (!ctx || !modes) return IQCP_ERR_ARG;
-  for (int i = 0; i < 2 * kNumPairClasses * kNumPairClasses; ++i) modes[i] = -1;
+  for (int i = 0; i < 4 * kNumPairClasses * kNumPairClasses; ++i) modes[i] = -1;
   for (const TaskRange& r : ctx->ranges)
     if (r.count > 0)
-      for (int kind = 0; kind < 2; ++kind)
-        modes[(kind * kNumPairClasses + r.X) * kNumPairClasses + r.Y] = r.mode[kind];
+      for (int kind = 0; kind < 4; ++kind)
+        modes[(kind * kNumPairClasses + r.X) * kNumPairClasses + r.Y] =
+            kind < 2 ? r.mode[kind] : (r.split[kind - 2] ? r.mode32[kind - 2] : kNumModes);
   return IQCP_OK;
 }
 
 int iqcp_set_kernel_mode(iqcp_ctx* ctx, int kind, int X, int Y, int mode) {
-  if (!ctx || kind < 0 || kind > 1 || mode < 0 || mode >= kNumModes) return IQCP_ERR_ARG;
-  for (TaskRange& r : ctx->ranges)
-    if ((X < 0 || r.X == X) && (Y < 0 || r.Y == Y)) r.mode[kind] = mode;
+  if (!ctx || kind < 0 || kind > 3 || mode < 0 || mode > kNumModes || (kind < 2 && mode == kNumModes))
+    return IQCP_ERR_ARG;
+  for (TaskRange& r : ctx->ranges) {
+    if (!((X < 0 || r.X == X) && (Y < 0 || r.Y == Y))) continue;
+    if (kind < 2) {
+      r.mode[kind] = mode;
+    } else if (mode == kNumModes) {
+      r.split[kind - 2] = 0;
+    } else {
+      r.split[kind - 2] = 1;
+      r.mode32[kind - 2] = mode;
+    }
+  }
   return IQCP_OK;
 }
 

@@ -116,3 +116,16 @@ def test_batch_single_geometry_only_calls():
             eng.eri_compressed()
         rc = eng._lib.iqcp_eri_compressed(eng._h, None, 0)
         assert rc != 0
+
+
+def test_batch_rhf_gradient_match_single():
+    bases = _mixed_bases()[:4]
+    Ds = [random_density(b.n_basis, 600 + i, 0.3) for i, b in enumerate(bases)]
+    Ws = [random_density(b.n_basis, 700 + i, 0.3) for i, b in enumerate(bases)]
+    with BatchFockEngine(bases) as beng:
+        g1b = beng.one_electron_gradient(Ds, Ws)
+        gb = beng.rhf_gradient(Ds, Ws)
+    for b, D, W, g1, g in zip(bases, Ds, Ws, g1b, gb):
+        with FockEngine(b) as eng:
+            assert np.abs(g1 - eng.one_electron_gradient(D, W)).max() < 1e-10
+            assert np.abs(g - eng.rhf_gradient(D, W)).max() < 1e-10
