@@ -31,6 +31,8 @@ METRIC = "Fock J/K builds/s + gradient evals/s, mixed vs FP64 at ≤1 µHa / ≤
 UNIT = "steps/s (1 J/K build + 1 gradient eval)"
 WORKLOAD = "c2"
 L2_FLUSH_BYTES = 256 << 20
+MIXED_CUTOFF = 1e-2          # Schwarz x density bound below which quartets run in FP32
+BATCH_SIZE = 64              # geometries of the batched measurement (8-48 atoms, H-Cl, 6-31G*)
 
 
 def parse():
@@ -43,6 +45,10 @@ def parse():
     ap.add_argument("--cpu-sample-stride", type=int, default=16,
                     help="oracle CPU baseline evaluates every stride-th bra shell pair")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch", type=int, default=BATCH_SIZE,
+                    help="geometries in the batched measurement (0: skip)")
+    ap.add_argument("--batch-scf", action="store_true",
+                    help="also run the batched device SCF + gradients to convergence")
     return ap.parse_args()
 
 
@@ -126,6 +132,127 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": reasons, "samples": len(rows),
                 "power_w_max": max((float(r[3]) for r in rows if r[3].replace(".", "").isdigit()), default=None)}
+
+
+def timed_steps(step, steps, flush, stream):
+    """Device time (ms) of `steps` calls of step(), L2 flushed before each."""
+    import torch
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    torch.cuda.synchronize()
+    for k in range(steps):
+        flush.zero_()
+        ev[k][0].record(stream)
+        step()
+        ev[k][1].record(stream)
+    torch.cuda.synchronize()
+    return sum(a.elapsed_time(b_) for a, b_ in ev)
+
+
+def measure_mixed(args, eng, b, H, D, dD, dJ, dK, dg, flush, stream, world):
+    """The mixed form at MIXED_CUTOFF: FP32 quadrature for quartets whose
+    Schwarz x density bound is below it (autotuned split per class), timed like
+    the FP64 step, with its energy, Fock and gradient errors against FP64."""
+    import torch
+    import torch.distributed as dist
+    from iqcp_b200 import FP64, MIXED
+    F64 = eng.build_fock(H, D)
+    g64 = eng.eri_gradient(D, 1.0)
+    e64 = 0.5 * float(np.sum(D * (H + F64)))
+    eng.set_precision(MIXED, MIXED_CUTOFF)
+    eng.autotune(dD.data_ptr(), 2)
+
+    def step():
+        eng.jk_device(dD.data_ptr(), dJ.data_ptr(), dK.data_ptr())
+        dg.zero_()
+        eng.eri_gradient_device(dD.data_ptr(), 1.0, dg.data_ptr())
+
+    for _ in range(args.warmup):
+        step()
+    t_ms = timed_steps(step, args.steps, flush, stream)
+    if world > 1:
+        tt = torch.tensor([t_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_ms = float(tt.item())
+    eng.jk_device(dD.data_ptr(), dJ.data_ptr(), dK.data_ptr())
+    nq = eng.last_stats()
+    eng.eri_gradient_device(dD.data_ptr(), 1.0, dg.data_ptr())
+    ng = eng.last_stats()
+    F = eng.build_fock(H, D)
+    g = eng.eri_gradient(D, 1.0)
+    e = 0.5 * float(np.sum(D * (H + F)))
+    modes = eng.kernel_modes()
+    eng.set_precision(FP64)
+    de, dgmax = abs(e - e64), float(np.abs(g - g64).max())
+    return {"cutoff": MIXED_CUTOFF, "value": world * args.steps / (t_ms * 1e-3), "unit": UNIT,
+            "ms_per_step": t_ms / args.steps,
+            "energy_error_ha": de, "fock_max_error_ha": float(np.abs(F - F64).max()),
+            "grad_max_error_ha_bohr": dgmax, "within_bounds": bool(de <= 1e-6 and dgmax <= 1e-6),
+            "fp32_quartet_share_jk": nq["fp32_quartets"] / max(nq["quartets"], 1),
+            "fp32_quartet_share_grad": ng["fp32_quartets"] / max(ng["quartets"], 1),
+            "split_classes": {"jk": int(((modes[2] >= 0) & (modes[2] < 4)).sum()),
+                              "grad": int(((modes[3] >= 0) & (modes[3] < 4)).sum()), "of": 21},
+            "note": "FP32 quadrature (FP64 roots, weights, accumulation) for quartets with "
+                    "Q_ij Q_kl max|D| (gradient: max|D|^2) below the cutoff, in the classes where the autotuner "
+                    "found the FP64/FP32 split faster than FP64 alone; errors against the FP64 form at the same "
+                    "density"}
+
+
+def measure_batch(args):
+    """Batched context: BATCH_SIZE seeded geometries of uneven size through one
+    context; one step = one J/K build + one gradient of every geometry."""
+    import torch
+    from iqcp_b200 import BasisSet
+    from iqcp_b200.batch_scf import BatchRHF
+    from iqcp_b200.molecules import batch_geometries
+    t0 = time.perf_counter()
+    geoms = batch_geometries(args.batch, seed=args.seed)
+    bases = [BasisSet.build(a, "6-31g*") for a in geoms]
+    scf = BatchRHF(bases)          # packed H, core-guess densities, batched context
+    eng = scf.eng
+    stream = torch.cuda.current_stream()
+    eng.set_stream(stream.cuda_stream)
+    eng.autotune(scf.D_p.data_ptr(), 1)
+    setup_s = time.perf_counter() - t0
+    J = torch.empty_like(scf.D_p)
+    K = torch.empty_like(scf.D_p)
+    g = torch.zeros((eng.n_atoms, 3), dtype=torch.float64, device="cuda")
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+
+    def jk():
+        eng.jk_device(scf.D_p.data_ptr(), J.data_ptr(), K.data_ptr())
+
+    def grad():
+        g.zero_()
+        eng.eri_gradient_device(scf.D_p.data_ptr(), 1.0, g.data_ptr())
+
+    jk()
+    grad()
+    steps = max(1, min(args.steps, 3))
+    tj = timed_steps(jk, steps, flush, stream) / steps
+    tg = timed_steps(grad, steps, flush, stream) / steps
+    nbf = np.array([bb.n_basis for bb in bases])
+    out = {"geometries": args.batch, "basis": "6-31g*", "atoms": [int(min(len(a) for a in geoms)),
+                                                                 int(max(len(a) for a in geoms))],
+           "nbf_total": int(nbf.sum()), "nbf_range": [int(nbf.min()), int(nbf.max())],
+           "jk_ms": tj, "grad_ms": tg, "jk_builds_per_s": args.batch / (tj * 1e-3),
+           "grad_evals_per_s": args.batch / (tg * 1e-3),
+           "geometry_steps_per_s": args.batch / ((tj + tg) * 1e-3), "setup_s": setup_s,
+           "density": "core-Hamiltonian guess of each geometry (J/K cost depends on the Schwarz lists, not D)"}
+    if args.batch_scf:
+        t1 = time.perf_counter()
+        res = scf.run()
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        scf.gradients()
+        torch.cuda.synchronize()
+        t3 = time.perf_counter()
+        out["scf"] = {"iterations": res.iterations, "converged": int(res.converged.sum()),
+                      "scf_s": t2 - t1, "gradient_s": t3 - t2,
+                      "geometries_per_s": args.batch / (t3 - t1),
+                      "note": "RHF to dE 1e-9, rms dD 1e-7, DIIS error 1e-5; one CUDA graph per iteration "
+                              "(Fock build, DIIS, purification); energy + gradient per geometry"}
+    scf.eng.close()
+    return out
 
 
 def run_reference(args, rank):
@@ -269,6 +396,11 @@ def main():
            "h2d_bytes_per_step": 2 * n * n * 8 + b.n_atoms * 3 * 8,
            "d2h_bytes_per_step": 2 * n * n * 8 + b.n_atoms * 3 * 8}
 
+    mixed = measure_mixed(args, eng, b, H, D, dD, dJ, dK, dg, flush, stream, world)
+    batch = None
+    if world == 1 and args.batch > 0:
+        batch = measure_batch(args)
+
     # roofline of the dominant quartet kernel (FP64 pipe)
     fl_jk, pq_jk, q_jk = eng.model_flops("jk")
     fl_gr, pq_gr, q_gr = eng.model_flops("grad")
@@ -310,6 +442,9 @@ def main():
     gr_ms = sum(v[0] / v[1] for k, v in per_kernel.items() if k[0] == "grad")
     line["jk_builds_per_s_fp64"] = 1e3 / jk_ms
     line["grad_evals_per_s_fp64"] = 1e3 / gr_ms
+    line["mixed"] = mixed
+    if batch is not None:
+        line["batch"] = batch
     if cpu is not None:
         line["cpu_baseline"] = cpu
     if rank == 0:

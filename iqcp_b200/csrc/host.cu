@@ -1065,6 +1065,10 @@ int iqcp_autotune(iqcp_ctx* ctx, const double* dD, int reps) {
   CK(cudaEventCreate(&e1));
   // best time over the variants of one (range, kind, pass); mode_out gets the winner
   auto tune = [&](TaskRange& r, int kind, int pass, int* mode_out, float* t_out) -> int {
+    // a batched context times a sample of the range: the tasks of about eight
+    // molecules' worth (tasks run molecule by molecule)
+    const int ntune = ctx->n_mol > 8 ? std::min(r.count, std::max(4096, int((long long)r.count * 8 / ctx->n_mol)))
+                                     : r.count;
     float best = 1e30f;
     for (int mode = 0; mode < kNumModes; ++mode) {
       if (pass == 2 && mode == 3) continue;  // the FP32 share has no 32-lane variant
@@ -1076,10 +1080,12 @@ int iqcp_autotune(iqcp_ctx* ctx, const double* dD, int reps) {
         CK(cudaMemsetAsync(ctx->d_counters, 0, sizeof(int), ctx->stream));
         CK(cudaEventRecord(e0, ctx->stream));
         if (kind == 0) {
-          const JKArgs a = jk_args(ctx, r, ctx->d_Ds, ctx->d_Jt, ctx->d_Kt, mode, pass, ctx->d_counters);
+          JKArgs a = jk_args(ctx, r, ctx->d_Ds, ctx->d_Jt, ctx->d_Kt, mode, pass, ctx->d_counters);
+          a.ntasks = ntune;
           CK(launch_jk(r.X, r.Y, a, ctx->stream));
         } else {
-          const GradArgs a = grad_args(ctx, r, ctx->d_Ds, 0.25, ctx->d_grad, mode, pass, ctx->d_counters);
+          GradArgs a = grad_args(ctx, r, ctx->d_Ds, 0.25, ctx->d_grad, mode, pass, ctx->d_counters);
+          a.ntasks = ntune;
           CK(launch_grad(r.X, r.Y, a, ctx->stream));
         }
         CK(cudaEventRecord(e1, ctx->stream));
