@@ -17,22 +17,24 @@ inline cudaError_t set_smem(K kernel, size_t bytes) {
 // by the work), each looping over tasks; per-block set-up (the staged Rys
 // table, the gradient accumulator) is then paid once per resident block.
 template <typename K>
-inline int persistent_blocks(K kernel, size_t smem, int ntasks) {
+inline int persistent_blocks(K kernel, size_t smem, int ntasks, int threads = 128) {
   int per_sm = 0, dev = 0, sms = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 128, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int need = (ntasks + 3) / 4;
+  const int wpb = threads / 32;
+  const int need = (ntasks + wpb - 1) / wpb;
   const int cap = (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
   return need < cap ? need : cap;
 }
 
-#define IQCP_LAUNCH(KERNEL, SMEM, ARGS, ST)                                      \
-  do {                                                                           \
-    cudaError_t e_ = set_smem(KERNEL, SMEM);                                     \
-    if (e_ != cudaSuccess) return e_;                                            \
-    KERNEL<<<persistent_blocks(KERNEL, SMEM, (ARGS).ntasks), 128, SMEM, ST>>>(ARGS); \
+#define IQCP_LAUNCH_T(KERNEL, THREADS, SMEM, ARGS, ST)                                             \
+  do {                                                                                             \
+    cudaError_t e_ = set_smem(KERNEL, SMEM);                                                       \
+    if (e_ != cudaSuccess) return e_;                                                              \
+    KERNEL<<<persistent_blocks(KERNEL, SMEM, (ARGS).ntasks, THREADS), THREADS, SMEM, ST>>>(ARGS); \
   } while (0)
+#define IQCP_LAUNCH(KERNEL, SMEM, ARGS, ST) IQCP_LAUNCH_T(KERNEL, 128, SMEM, ARGS, ST)
 
 // mode: 0 one quartet per thread, 1 warp-cooperative (eri_team.cuh),
 // 2 / 3 eight / thirty-two lanes share one quartet's primitive quartets
@@ -84,17 +86,18 @@ cudaError_t launch_grad_variant(const GradArgs& args, cudaStream_t st) {
   using C = Cls<LA, LB, LC, LD>;
   constexpr bool F32 = sizeof(R) == 4;
   constexpr int NRG = (LA + LB + LC + LD + 2) / 2 + 1;
+  using TG = TeamGrad2<LA, LB, LC, LD>;
   const bool team = args.mode == 1 || (F32 && C::NCOMP > 324);
-  const size_t fixed = sizeof(double) * rys_tab_doubles<NRG>() +
-                       (team ? sizeof(double) * 4 * TeamGrad<LA, LB, LC, LD>::PER_WARP : 0);
+  // the team variant reads the Rys coefficients through L1 (no staged table)
+  const size_t fixed = team ? sizeof(double) * TG::WPB * TG::PER_WARP : sizeof(double) * rys_tab_doubles<NRG>();
   // the per-block gradient accumulator only when it fits beside the tables
   GradArgs a = args;
   if (a.gsmem && fixed + sizeof(double) * 3 * a.natoms > max_smem_optin()) a.gsmem = 0;
   const size_t gacc = a.gsmem ? sizeof(double) * 3 * a.natoms : 0;
   const size_t tb = sizeof(double) * rys_tab_doubles<NRG>() + gacc;
   if (team) {
-    const size_t bytes = sizeof(double) * 4 * TeamGrad<LA, LB, LC, LD>::PER_WARP + tb;
-    IQCP_LAUNCH((grad_team_kernel<R, LA, LB, LC, LD>), bytes, a, st);
+    const size_t bytes = sizeof(double) * TG::WPB * TG::PER_WARP + gacc;
+    IQCP_LAUNCH_T((grad_team2_kernel<R, LA, LB, LC, LD>), 32 * TG::WPB, bytes, a, st);
   } else if (C::NCOMP <= 36 && (a.mode == 2 || a.mode == 3)) {
     if constexpr (C::NCOMP <= 36) {
       if (a.mode == 2 || F32) IQCP_LAUNCH((grad_kernel<R, LA, LB, LC, LD, 8>), tb, a, st);

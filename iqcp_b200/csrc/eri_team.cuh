@@ -243,70 +243,118 @@ __global__ void __launch_bounds__(128) jk_team_kernel(JKArgs args) {
 }
 
 // ---------------------------------------------------------------------------
-// Gradient team kernel.  Tables are extended by one on A, B and C (the D
-// derivative follows from translational invariance, dD = -(dA + dB + dC)),
-// with one more root than the energy (gradient.rs / eri/mod.rs:2146-2149).
+// Gradient team kernel with per-root derivative tables.
+//
+// Tables are extended by one on A, B and C (the D derivative follows from
+// translational invariance, dD = -(dA + dB + dC)), with one more root than the
+// energy (eri/mod.rs:2146-2149).  Per surviving primitive quartet:
+//   phase A   lanes 0 .. 3*NR-1 build the extended 1D tables E of their
+//             (root, axis) in shared memory;
+//   phase A2  all 32 lanes turn them into, for every unextended index
+//             (ia, ib, ic, id), the four values I, dI/dA, dI/dB, dI/dC
+//             (d/dA: 2a E(ia+1) - ia E(ia-1), likewise B, C), stored together;
+//   phase B   each lane accumulates its components c = lane + 32 m: per root
+//             two vector loads per axis and 15 flops for the nine A/B/C
+//             derivatives (instead of ~21 scattered loads when each lane
+//             forms the derivatives from E itself).
+// The Rys coefficients are read through L1 (the 3*NR lanes of a warp read one
+// T interval), so no table is staged per block, and the warps per block are
+// chosen so that the per-warp tables fit.
+template <int N>
+__device__ __forceinline__ void rys_rule_one_g(double T, int r, double* t2, double* w) {
+  constexpr int NI = rys_nint(N);
+  if (T >= double(NI)) {
+    const int base = (N * (N - 1)) / 2;
+    *t2 = __ldg(kRysAsymRoot + base + r) / T;
+    *w = __ldg(kRysAsymWeight + base + r) / sqrt(T);
+    return;
+  }
+  const int k = int(T);
+  const double x2 = 2.0 * (2.0 * (T - double(k)) - 1.0);
+  const double* c = kRysCheb + kRysOffset[N] + k * (2 * N * (RYS_TAB_DEG + 1));
+  *t2 = cheb_clenshaw(c + r * (RYS_TAB_DEG + 1), x2);
+  *w = cheb_clenshaw(c + (N + r) * (RYS_TAB_DEG + 1), x2);
+}
+
+// Warps per block for a per-warp shared footprint of `per_warp` doubles: the
+// choice of 4, 2, 1 with the most warps resident per SM (228 KB shared memory,
+// 1 KB reserved per block; at most 16 counted, beyond which registers limit
+// anyway), ties to the larger block.
+__host__ __device__ constexpr int team_resident(int w, int per_warp) {
+  return w * ((228 * 1024) / (w * per_warp * 8 + 1024)) < 16 ? w * ((228 * 1024) / (w * per_warp * 8 + 1024)) : 16;
+}
+__host__ __device__ constexpr int team_warps_per_block(int per_warp) {
+  return (team_resident(4, per_warp) >= team_resident(2, per_warp) &&
+          team_resident(4, per_warp) >= team_resident(1, per_warp) && team_resident(4, per_warp) > 0)
+             ? 4
+             : (team_resident(2, per_warp) >= team_resident(1, per_warp) && team_resident(2, per_warp) > 0 ? 2 : 1);
+}
+
 template <int LA, int LB, int LC, int LD>
-struct TeamGrad {
+struct TeamGrad2 {
   using C = Cls<LA, LB, LC, LD>;
   static constexpr int EA = LA + 1, EB = LB + 1, EC = LC + 1, ED = LD;
   static constexpr int NR = (LA + LB + LC + LD + 2) / 2 + 1;
   static constexpr int TSZ = (EA + 1) * (EB + 1) * (EC + 1) * (ED + 1);
   static constexpr int SA = (EB + 1) * (EC + 1) * (ED + 1), SB = (EC + 1) * (ED + 1), SC = ED + 1;
-  static constexpr int TAB = NR * 3 * TSZ;
+  static constexpr int RSZ = (LA + 1) * (LB + 1) * (LC + 1) * (LD + 1);
+  static constexpr int NT = 3 * NR;                       // (root, axis) tables
+  static constexpr int TAB = ((NT * TSZ + 3) / 4) * 4;    // extended tables (doubles, padded)
+  static constexpr int QT = NT * RSZ * 4;                 // I, dA, dB, dC per unextended entry
   static constexpr int DBLK = C::NA * C::NB + C::NC * C::ND + C::NA * C::NC + C::NB * C::ND + C::NA * C::ND +
                               C::NB * C::NC;
-  static constexpr int PER_WARP = TAB + DBLK;
+  static constexpr int PER_WARP = TAB + QT + ((DBLK + 3) / 4) * 4;
   static constexpr int CPL = (C::NCOMP + 31) / 32;
+  static constexpr int WPB = team_warps_per_block(PER_WARP);
   __host__ __device__ static constexpr int eidx(int a, int b, int c, int d) {
     return ((a * (EB + 1) + b) * (EC + 1) + c) * (ED + 1) + d;
   }
+  __host__ __device__ static constexpr int ridx(int a, int b, int c, int d) {
+    return ((a * (LB + 1) + b) * (LC + 1) + c) * (LD + 1) + d;
+  }
 };
 
+template <typename T> struct Vec2;
+template <> struct Vec2<double> { using type = double2; };
+template <> struct Vec2<float> { using type = float2; };
+
 template <typename R, int LA, int LB, int LC, int LD>
-__global__ void __launch_bounds__(128) grad_team_kernel(GradArgs args) {
+__global__ void __launch_bounds__(32 * TeamGrad2<LA, LB, LC, LD>::WPB) grad_team2_kernel(GradArgs args) {
   using C = Cls<LA, LB, LC, LD>;
-  using TG = TeamGrad<LA, LB, LC, LD>;
-  constexpr int NR = TG::NR, TSZ = TG::TSZ, CPL = TG::CPL;
-  constexpr bool F32 = sizeof(R) == 4;
-  extern __shared__ double smem[];
-  double* rtab = smem;
-  rys_stage_table<NR>(rtab);
-  __syncthreads();
+  using TG = TeamGrad2<LA, LB, LC, LD>;
+  using V2 = typename Vec2<R>::type;
+  constexpr int NR = TG::NR, TSZ = TG::TSZ, RSZ = TG::RSZ, CPL = TG::CPL;
+  extern __shared__ __align__(16) double smem[];
   const int wib = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
-  double* wbase = smem + rys_tab_doubles<NR>() + wib * TG::PER_WARP;
-  R* tab = reinterpret_cast<R*>(wbase);  // TAB entries of R (the region is sized for double)
-  double* gacc = smem + rys_tab_doubles<NR>() + 4 * TG::PER_WARP;
+  double* wbase = smem + wib * TG::PER_WARP;
+  R* tab = reinterpret_cast<R*>(wbase);
+  R* qt = reinterpret_cast<R*>(wbase + TG::TAB);
+  double* gacc = smem + TG::WPB * TG::PER_WARP;
   if (args.gsmem)
     for (int i = threadIdx.x; i < 3 * args.natoms; i += blockDim.x) gacc[i] = 0.0;
   __syncthreads();
   double* gout = args.gsmem ? gacc : args.grad;
-  double* Dab = wbase + TG::TAB;
+  double* Dab = wbase + TG::TAB + TG::QT;
   double* Dcd = Dab + C::NA * C::NB;
   double* Dac = Dcd + C::NC * C::ND;
   double* Dbd = Dac + C::NA * C::NC;
   double* Dad = Dbd + C::NB * C::ND;
   double* Dbc = Dad + C::NA * C::ND;
 
-  // packed per-component data: table offsets (3 x 8 bits) and A/B/C powers (9 x 2 bits)
-  int offs[CPL], pows[CPL];
+  // unextended table index of this lane's components, 7 bits per axis
+  int roffs[CPL];
 #pragma unroll
   for (int m = 0; m < CPL; ++m) {
     int comp = lane + 32 * m;
     if (comp >= C::NCOMP) comp = 0;
     const int d = comp % C::ND, c = (comp / C::ND) % C::NC, b = (comp / (C::ND * C::NC)) % C::NB,
               a = comp / (C::ND * C::NC * C::NB);
-    int o = 0, pw = 0;
+    int o = 0;
 #pragma unroll
-    for (int ax = 0; ax < 3; ++ax) {
-      const int ia = cart_pow(LA, a, ax), ib = cart_pow(LB, b, ax), ic = cart_pow(LC, c, ax),
-                id = cart_pow(LD, d, ax);
-      o |= (ax * TSZ + TG::eidx(ia, ib, ic, id)) << (10 * ax);
-      pw |= (ia | (ib << 2) | (ic << 4)) << (6 * ax);
-    }
-    offs[m] = o;
-    pows[m] = pw;
+    for (int ax = 0; ax < 3; ++ax)
+      o |= TG::ridx(cart_pow(LA, a, ax), cart_pow(LB, b, ax), cart_pow(LC, c, ax), cart_pow(LD, d, ax)) << (7 * ax);
+    roffs[m] = o;
   }
 
   for (int warp = next_task(args.next_task, lane); warp < args.ntasks; warp = next_task(args.next_task, lane)) {
@@ -322,7 +370,7 @@ __global__ void __launch_bounds__(128) grad_team_kernel(GradArgs args) {
     Dab[i] = __ldg(D + (bp.oa + i / C::NB) * n + bp.ob + i % C::NB);
   const bool ij_same = bp.sa == bp.sb;
   const double xs = args.xscale;
-  int nf32 = 0;
+  int nsel = 0;
   const unsigned sel = task_sel(args.mx, warp, task.nket);
 
   for (int kk = 0; kk < task.nket; ++kk) {
@@ -333,7 +381,7 @@ __global__ void __launch_bounds__(128) grad_team_kernel(GradArgs args) {
     // composite index) is below threshold (gradient.rs:1457-1460)
     const double qref = bp.comp >= kp.comp ? bp.Q : kp.Q;
     if (qref < args.schwarz_thr) continue;
-    ++nf32;
+    ++nsel;
     const bool kl_same = kp.sa == kp.sb;
     const bool bk_same = task.diag && kpos == task.bra_pos;
     for (int i = lane; i < C::NC * C::ND; i += 32) Dcd[i] = __ldg(D + (kp.oa + i / C::ND) * n + kp.ob + i % C::ND);
@@ -355,15 +403,15 @@ __global__ void __launch_bounds__(128) grad_team_kernel(GradArgs args) {
         const double dac = Dac[a * C::NC + c], dbd = Dbd[b * C::ND + d];
         const double dad = Dad[a * C::ND + d], dbc = Dbc[b * C::NC + c];
         // w(p,q,r,s) = 1/2 D_pq D_rs - xs D_pr D_qs over the distinct permutations
-        t = 0.5 * dab * dcd - xs * dac * dbd;                       // (ij|kl)
-        if (!ij_same) t += 0.5 * dab * dcd - xs * dbc * dad;        // (ji|kl)
-        if (!kl_same) t += 0.5 * dab * dcd - xs * dad * dbc;        // (ij|lk)
-        if (!ij_same && !kl_same) t += 0.5 * dab * dcd - xs * dbd * dac;  // (ji|lk)
+        t = 0.5 * dab * dcd - xs * dac * dbd;
+        if (!ij_same) t += 0.5 * dab * dcd - xs * dbc * dad;
+        if (!kl_same) t += 0.5 * dab * dcd - xs * dad * dbc;
+        if (!ij_same && !kl_same) t += 0.5 * dab * dcd - xs * dbd * dac;
         if (!bk_same) {
-          t += 0.5 * dcd * dab - xs * dac * dbd;                     // (kl|ij)
-          if (!kl_same) t += 0.5 * dcd * dab - xs * dad * dbc;       // (lk|ij)
-          if (!ij_same) t += 0.5 * dcd * dab - xs * dbc * dad;       // (kl|ji)
-          if (!ij_same && !kl_same) t += 0.5 * dcd * dab - xs * dbd * dac;  // (lk|ji)
+          t += 0.5 * dcd * dab - xs * dac * dbd;
+          if (!kl_same) t += 0.5 * dcd * dab - xs * dad * dbc;
+          if (!ij_same) t += 0.5 * dcd * dab - xs * dbc * dad;
+          if (!ij_same && !kl_same) t += 0.5 * dcd * dab - xs * dbd * dac;
         }
         const double angp = ang_factor(LA, a) * ang_factor(LB, b) * ang_factor(LC, c) * ang_factor(LD, d);
         if (fabs(t / angp) < 1e-15) t = 0.0;  // |w| < 1e-15 skip on the reference weight
@@ -385,10 +433,10 @@ __global__ void __launch_bounds__(128) grad_team_kernel(GradArgs args) {
           const double p = pb.p, q = pk.p, s = p + q;
           const double PQ[3] = {pb.P[0] - pk.P[0], pb.P[1] - pk.P[1], pb.P[2] - pk.P[2]};
           const double inv_s = 1.0 / s;
-        const double rho = p * q * inv_s;
+          const double rho = p * q * inv_s;
           const double T = rho * (PQ[0] * PQ[0] + PQ[1] * PQ[1] + PQ[2] * PQ[2]);
           double t2, wr;
-          rys_rule_one<NR>(T, r, rtab, &t2, &wr);
+          rys_rule_one_g<NR>(T, r, &t2, &wr);
           const double b00 = 0.5 * t2 * inv_s, h = 0.5 - 0.5 * t2;
           const double b10 = fma(h, pb.inv_p, b00), b01 = fma(h, pk.inv_p, b00);
           const double pa = pb.P[ax] - bp.A[ax], qc = pk.P[ax] - kp.A[ax];
@@ -398,67 +446,66 @@ __global__ void __launch_bounds__(128) grad_team_kernel(GradArgs args) {
               R(CD[ax]), R(g00), tab + (r * 3 + ax) * TSZ);
         }
         __syncwarp();
-        const R e2[3] = {R(2.0 * pb.aa), R(2.0 * (pb.p - pb.aa)), R(2.0 * pk.aa)};
-        const int str[3] = {TG::SA, TG::SB, TG::SC};
-        // FP32 share: this primitive quartet's derivatives in R, then added to the FP64 sums
-        R gp[F32 ? 9 : 1];
-        if constexpr (F32) {
-#pragma unroll
-          for (int x = 0; x < 9; ++x) gp[x] = R(0);
-        }
-#pragma unroll
-        for (int m = 0; m < CPL; ++m) {
-          const R w = R(W[m]);
-          if (W[m] == 0.0) continue;
-          const int o = offs[m], pw = pows[m];
-#pragma unroll
-          for (int r = 0; r < NR; ++r) {
-            const R* t = tab + r * 3 * TSZ;
-            int ox[3];
-            R reg[3];
-#pragma unroll
-            for (int ax = 0; ax < 3; ++ax) {
-              ox[ax] = (o >> (10 * ax)) & 0x3ff;
-              reg[ax] = t[ox[ax]];
-            }
-            const R wyz = w * reg[1] * reg[2], wxz = w * reg[0] * reg[2], wxy = w * reg[0] * reg[1];
-            const R wo[3] = {wyz, wxz, wxy};
-#pragma unroll
-            for (int ax = 0; ax < 3; ++ax) {
-#pragma unroll
-              for (int cen = 0; cen < 3; ++cen) {
-                const int pcen = (pw >> (6 * ax + 2 * cen)) & 3;
-                const R up = t[ox[ax] + str[cen]];
-                // power 0 has no lowered term; the index is clamped so no load leaves the table
-                const R dn = R(pcen) * t[pcen ? ox[ax] - str[cen] : ox[ax]];
-                if constexpr (F32) gp[3 * cen + ax] = fmaf(wo[ax], e2[cen] * up - dn, gp[3 * cen + ax]);
-                else g[3 * cen + ax] = fma(wo[ax], e2[cen] * up - dn, g[3 * cen + ax]);
-              }
-            }
+        // phase A2: I, dI/dA, dI/dB, dI/dC on the unextended indices
+        {
+          const R e2a = R(2.0 * pb.aa), e2b = R(2.0 * (pb.p - pb.aa)), e2c = R(2.0 * pk.aa);
+          for (int it = lane; it < 3 * NR * RSZ; it += 32) {
+            const int t = it / RSZ, e = it - t * RSZ;
+            const int d = e % (LD + 1), c = (e / (LD + 1)) % (LC + 1), b = (e / ((LD + 1) * (LC + 1))) % (LB + 1),
+                      a = e / ((LD + 1) * (LC + 1) * (LB + 1));
+            const R* E = tab + t * TSZ;
+            const int x = TG::eidx(a, b, c, d);
+            R* q = qt + (t * RSZ + e) * 4;
+            // power 0 has no lowered term; the index is clamped so no load leaves the table
+            q[0] = E[x];
+            q[1] = e2a * E[x + TG::SA] - R(a) * E[a ? x - TG::SA : x];
+            q[2] = e2b * E[x + TG::SB] - R(b) * E[b ? x - TG::SB : x];
+            q[3] = e2c * E[x + TG::SC] - R(c) * E[c ? x - TG::SC : x];
           }
         }
-        if constexpr (F32) {
+        __syncwarp();
+        R gl[9];
 #pragma unroll
-          for (int x = 0; x < 9; ++x) g[x] += double(gp[x]);
+        for (int x = 0; x < 9; ++x) gl[x] = R(0);
+#pragma unroll
+        for (int m = 0; m < CPL; ++m) {
+          if (W[m] == 0.0) continue;
+          const R w = R(W[m]);
+          const int o = roffs[m];
+#pragma unroll
+          for (int r = 0; r < NR; ++r) {
+            V2 v0[3], v1[3];
+#pragma unroll
+            for (int ax = 0; ax < 3; ++ax) {
+              const V2* q = reinterpret_cast<const V2*>(qt + ((r * 3 + ax) * RSZ + ((o >> (7 * ax)) & 127)) * 4);
+              v0[ax] = q[0];  // I, dI/dA
+              v1[ax] = q[1];  // dI/dB, dI/dC
+            }
+            const R wyz = w * v0[1].x * v0[2].x, wxz = w * v0[0].x * v0[2].x, wxy = w * v0[0].x * v0[1].x;
+            gl[0] = fma(wyz, v0[0].y, gl[0]); gl[1] = fma(wxz, v0[1].y, gl[1]); gl[2] = fma(wxy, v0[2].y, gl[2]);
+            gl[3] = fma(wyz, v1[0].x, gl[3]); gl[4] = fma(wxz, v1[1].x, gl[4]); gl[5] = fma(wxy, v1[2].x, gl[5]);
+            gl[6] = fma(wyz, v1[0].y, gl[6]); gl[7] = fma(wxz, v1[1].y, gl[7]); gl[8] = fma(wxy, v1[2].y, gl[8]);
+          }
         }
+#pragma unroll
+        for (int x = 0; x < 9; ++x) g[x] += double(gl[x]);
       }
     }
     // warp reduction of the nine derivatives, then atomics (D by invariance)
 #pragma unroll
     for (int x = 0; x < 9; ++x) g[x] = warp_sum(g[x]);
     if (lane == 0) {
-      double* gr = gout;
 #pragma unroll
       for (int ax = 0; ax < 3; ++ax) {
-        atomicAdd(gr + 3 * bp.atom_a + ax, g[ax]);
-        atomicAdd(gr + 3 * bp.atom_b + ax, g[3 + ax]);
-        atomicAdd(gr + 3 * kp.atom_a + ax, g[6 + ax]);
-        atomicAdd(gr + 3 * kp.atom_b + ax, -(g[ax] + g[3 + ax] + g[6 + ax]));
+        atomicAdd(gout + 3 * bp.atom_a + ax, g[ax]);
+        atomicAdd(gout + 3 * bp.atom_b + ax, g[3 + ax]);
+        atomicAdd(gout + 3 * kp.atom_a + ax, g[6 + ax]);
+        atomicAdd(gout + 3 * kp.atom_b + ax, -(g[ax] + g[3 + ax] + g[6 + ax]));
       }
     }
     __syncwarp();
   }
-  if (F32 && lane == 0 && args.mx.fp32_count && nf32) atomicAdd(args.mx.fp32_count, (unsigned long long)nf32);
+  if (sizeof(R) == 4 && lane == 0 && args.mx.fp32_count && nsel) atomicAdd(args.mx.fp32_count, (unsigned long long)nsel);
   }  // task loop
   if (args.gsmem) {
     __syncthreads();
