@@ -47,6 +47,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch", type=int, default=BATCH_SIZE,
                     help="geometries in the batched measurement (0: skip)")
+    ap.add_argument("--modes", default="",
+                    help="force kernel variants instead of autotuning, e.g. 'jk:0,grad:1' (for profiling runs)")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-form measurement")
     ap.add_argument("--batch-scf", action="store_true",
                     help="also run the batched device SCF + gradients to convergence")
     return ap.parse_args()
@@ -341,7 +344,13 @@ def main():
         return l1 + l2 + 1, p1 + p2
 
     # kernel variant per class, picked on this density (set-up, not timed)
-    modes = eng.autotune(dD.data_ptr(), 2)
+    if args.modes:
+        for item in args.modes.split(","):
+            kind, m = item.split(":")
+            eng.set_kernel_mode(kind, mode=int(m))
+        modes = eng.kernel_modes()
+    else:
+        modes = eng.autotune(dD.data_ptr(), 2)
     for _ in range(args.warmup):
         step()
     eng.set_profiling(True)
@@ -396,7 +405,7 @@ def main():
            "h2d_bytes_per_step": 2 * n * n * 8 + b.n_atoms * 3 * 8,
            "d2h_bytes_per_step": 2 * n * n * 8 + b.n_atoms * 3 * 8}
 
-    mixed = measure_mixed(args, eng, b, H, D, dD, dJ, dK, dg, flush, stream, world)
+    mixed = None if args.no_mixed else measure_mixed(args, eng, b, H, D, dD, dJ, dK, dg, flush, stream, world)
     batch = None
     if world == 1 and args.batch > 0:
         batch = measure_batch(args)
@@ -442,7 +451,8 @@ def main():
     gr_ms = sum(v[0] / v[1] for k, v in per_kernel.items() if k[0] == "grad")
     line["jk_builds_per_s_fp64"] = 1e3 / jk_ms
     line["grad_evals_per_s_fp64"] = 1e3 / gr_ms
-    line["mixed"] = mixed
+    if mixed is not None:
+        line["mixed"] = mixed
     if batch is not None:
         line["batch"] = batch
     if cpu is not None:

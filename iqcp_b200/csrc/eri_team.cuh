@@ -252,7 +252,8 @@ __global__ void __launch_bounds__(128) jk_team_kernel(JKArgs args) {
 //             (root, axis) in shared memory;
 //   phase A2  all 32 lanes turn them into, for every unextended index
 //             (ia, ib, ic, id), the four values I, dI/dA, dI/dB, dI/dC
-//             (d/dA: 2a E(ia+1) - ia E(ia-1), likewise B, C), stored together;
+//             (d/dA: 2a E(ia+1) - ia E(ia-1), likewise B, C), stored as two
+//             planes of pairs (I, dA) and (dB, dC);
 //   phase B   each lane accumulates its components c = lane + 32 m: per root
 //             two vector loads per axis and 15 flops for the nine A/B/C
 //             derivatives (instead of ~21 scattered loads when each lane
@@ -455,12 +456,15 @@ __global__ void __launch_bounds__(32 * TeamGrad2<LA, LB, LC, LD>::WPB) grad_team
                       a = e / ((LD + 1) * (LC + 1) * (LB + 1));
             const R* E = tab + t * TSZ;
             const int x = TG::eidx(a, b, c, d);
-            R* q = qt + (t * RSZ + e) * 4;
+            // two planes of pairs per table, (I, dA) and (dB, dC), 2 * sizeof(R) apart
+            // per entry, so that lanes reading different entries spread over the banks
+            R* q0 = qt + ((2 * t) * RSZ + e) * 2;
+            R* q1 = qt + ((2 * t + 1) * RSZ + e) * 2;
             // power 0 has no lowered term; the index is clamped so no load leaves the table
-            q[0] = E[x];
-            q[1] = e2a * E[x + TG::SA] - R(a) * E[a ? x - TG::SA : x];
-            q[2] = e2b * E[x + TG::SB] - R(b) * E[b ? x - TG::SB : x];
-            q[3] = e2c * E[x + TG::SC] - R(c) * E[c ? x - TG::SC : x];
+            q0[0] = E[x];
+            q0[1] = e2a * E[x + TG::SA] - R(a) * E[a ? x - TG::SA : x];
+            q1[0] = e2b * E[x + TG::SB] - R(b) * E[b ? x - TG::SB : x];
+            q1[1] = e2c * E[x + TG::SC] - R(c) * E[c ? x - TG::SC : x];
           }
         }
         __syncwarp();
@@ -477,9 +481,9 @@ __global__ void __launch_bounds__(32 * TeamGrad2<LA, LB, LC, LD>::WPB) grad_team
             V2 v0[3], v1[3];
 #pragma unroll
             for (int ax = 0; ax < 3; ++ax) {
-              const V2* q = reinterpret_cast<const V2*>(qt + ((r * 3 + ax) * RSZ + ((o >> (7 * ax)) & 127)) * 4);
-              v0[ax] = q[0];  // I, dI/dA
-              v1[ax] = q[1];  // dI/dB, dI/dC
+              const int t = r * 3 + ax, e = (o >> (7 * ax)) & 127;
+              v0[ax] = *reinterpret_cast<const V2*>(qt + ((2 * t) * RSZ + e) * 2);      // I, dI/dA
+              v1[ax] = *reinterpret_cast<const V2*>(qt + ((2 * t + 1) * RSZ + e) * 2);  // dI/dB, dI/dC
             }
             const R wyz = w * v0[1].x * v0[2].x, wxz = w * v0[0].x * v0[2].x, wxy = w * v0[0].x * v0[1].x;
             gl[0] = fma(wyz, v0[0].y, gl[0]); gl[1] = fma(wxz, v0[1].y, gl[1]); gl[2] = fma(wxy, v0[2].y, gl[2]);
