@@ -68,7 +68,7 @@ __device__ __forceinline__ void team_prim_loop(const JKArgs& args, const ShellPa
         const int r = lane / 3, ax = lane - 3 * r;
         const double p = pb.p, q = pk.p, s = p + q;
         const double PQ[3] = {pb.P[0] - pk.P[0], pb.P[1] - pk.P[1], pb.P[2] - pk.P[2]};
-        const double inv_s = 1.0 / s;
+        const double rs = rsqrt(s), inv_s = rs * rs;  // 1/(p+q), 1/sqrt(p+q): one rsqrt
         const double rho = p * q * inv_s;
         const double T = rho * (PQ[0] * PQ[0] + PQ[1] * PQ[1] + PQ[2] * PQ[2]);
         double t2, wr;
@@ -76,7 +76,7 @@ __device__ __forceinline__ void team_prim_loop(const JKArgs& args, const ShellPa
         const double b00 = 0.5 * t2 * inv_s, h = 0.5 - 0.5 * t2;
         const double b10 = fma(h, pb.inv_p, b00), b01 = fma(h, pk.inv_p, b00);
         const double pa = pb.P[ax] - bp.A[ax], qc = pk.P[ax] - kp.A[ax];
-        const double g00 = ax == 2 ? wr * kTwoPi52 * pb.cK * pk.cK * pb.inv_p * pk.inv_p * inv_s * sqrt(s) : 1.0;
+        const double g00 = ax == 2 ? wr * kTwoPi52 * pb.cK * pk.cK * pb.inv_p * pk.inv_p * rs : 1.0;
         axis_table<R, C::NBRA, C::NKET, LA, LB, LC, LD>(
             R(pa - t2 * q * inv_s * PQ[ax]), R(qc + t2 * p * inv_s * PQ[ax]), R(b00), R(b10), R(b01), R(AB[ax]),
             R(CD[ax]), R(g00), tab + (r * 3 + ax) * TSZ);
@@ -433,7 +433,7 @@ __global__ void __launch_bounds__(32 * TeamGrad2<LA, LB, LC, LD>::WPB) grad_team
           const int r = lane / 3, ax = lane - 3 * r;
           const double p = pb.p, q = pk.p, s = p + q;
           const double PQ[3] = {pb.P[0] - pk.P[0], pb.P[1] - pk.P[1], pb.P[2] - pk.P[2]};
-          const double inv_s = 1.0 / s;
+          const double rs = rsqrt(s), inv_s = rs * rs;  // 1/(p+q), 1/sqrt(p+q): one rsqrt
           const double rho = p * q * inv_s;
           const double T = rho * (PQ[0] * PQ[0] + PQ[1] * PQ[1] + PQ[2] * PQ[2]);
           double t2, wr;
@@ -441,7 +441,7 @@ __global__ void __launch_bounds__(32 * TeamGrad2<LA, LB, LC, LD>::WPB) grad_team
           const double b00 = 0.5 * t2 * inv_s, h = 0.5 - 0.5 * t2;
           const double b10 = fma(h, pb.inv_p, b00), b01 = fma(h, pk.inv_p, b00);
           const double pa = pb.P[ax] - bp.A[ax], qc = pk.P[ax] - kp.A[ax];
-          const double g00 = ax == 2 ? wr * kTwoPi52 * pb.cK * pk.cK * pb.inv_p * pk.inv_p * inv_s * sqrt(s) : 1.0;
+          const double g00 = ax == 2 ? wr * kTwoPi52 * pb.cK * pk.cK * pb.inv_p * pk.inv_p * rs : 1.0;
           axis_table<R, LA + LB + 1, LC + LD + 1, TG::EA, TG::EB, TG::EC, TG::ED>(
               R(pa - t2 * q * inv_s * PQ[ax]), R(qc + t2 * p * inv_s * PQ[ax]), R(b00), R(b10), R(b01), R(AB[ax]),
               R(CD[ax]), R(g00), tab + (r * 3 + ax) * TSZ);

@@ -144,10 +144,10 @@ __device__ __forceinline__ void quartet(const ShellPair& bp, const ShellPair& kp
     if (b.K * k.K < thr) continue;
     const double p = b.p, q = k.p, s = p + q;
     const double PQ[3] = {b.P[0] - k.P[0], b.P[1] - k.P[1], b.P[2] - k.P[2]};
-    const double inv_s = 1.0 / s;
+    const double rs = rsqrt(s), inv_s = rs * rs;  // 1/(p+q), 1/sqrt(p+q): one rsqrt
     const double rho = p * q * inv_s;
     const double T = rho * (PQ[0] * PQ[0] + PQ[1] * PQ[1] + PQ[2] * PQ[2]);
-    const double pref = kTwoPi52 * b.cK * k.cK * b.inv_p * k.inv_p * inv_s * sqrt(s);
+    const double pref = kTwoPi52 * b.cK * k.cK * b.inv_p * k.inv_p * rs;
     double rt[C::NR], wt[C::NR];
     if (rtab) rys_rule_tab<C::NR>(T, rtab, rt, wt);
     else rys_rule<C::NR>(T, rt, wt);
@@ -510,10 +510,10 @@ __global__ void __launch_bounds__(128, (LA + LB + LC + LD <= 1) ? 4 : 1) grad_ke
         if (b.K * k.K < args.prim_thr) continue;
         const double p = b.p, q = k.p, s = p + q;
         const double PQ[3] = {b.P[0] - k.P[0], b.P[1] - k.P[1], b.P[2] - k.P[2]};
-        const double inv_s = 1.0 / s;
+        const double rs = rsqrt(s), inv_s = rs * rs;  // 1/(p+q), 1/sqrt(p+q): one rsqrt
         const double rho = p * q * inv_s;
         const double T = rho * (PQ[0] * PQ[0] + PQ[1] * PQ[1] + PQ[2] * PQ[2]);
-        const double pref = kTwoPi52 * b.cK * k.cK * b.inv_p * k.inv_p * inv_s * sqrt(s);
+        const double pref = kTwoPi52 * b.cK * k.cK * b.inv_p * k.inv_p * rs;
         double rt[NR], wt[NR];
         rys_rule_tab<NR>(T, rtab, rt, wt);
         const double PA[3] = {b.P[0] - bp.A[0], b.P[1] - bp.A[1], b.P[2] - bp.A[2]};

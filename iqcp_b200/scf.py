@@ -16,17 +16,27 @@ class ScfResult:
         self.__dict__.update(kw)
 
 
-def _orthogonalizer(S):
+def _orthogonalizer(S, lindep=None):
+    """Symmetric S^-1/2 (build_orthogonalizer, scf/mod.rs:709-735: error at
+    eigenvalues <= 1e-10).  With lindep set and the smallest eigenvalue below
+    it, canonical orthogonalisation instead: the eigenvectors with eigenvalues
+    below lindep are dropped (X is nbf x nkept), which keeps near-linearly
+    dependent diffuse bases (large molecules in 6-31+G*) from amplifying
+    rounding into the orthogonal basis.  Off by default, as in the reference."""
     w, U = np.linalg.eigh(S)
-    if w.min() <= 1e-10:
+    if w.min() <= 1e-10 and lindep is None:
         raise ValueError("overlap matrix is singular")
+    if lindep is not None and w.min() < lindep:
+        keep = w >= lindep
+        return U[:, keep] / np.sqrt(w[keep])
     return (U / np.sqrt(w)) @ U.T
 
 
 def rhf_scf(S, H, e_nuc, n_occ, build_fock, e_tol=1e-10, d_tol=1e-8, max_iter=100, diis_size=8,
-            use_diis=True, D0=None):
-    """Restricted Hartree-Fock; build_fock(H, D) -> F.  Returns ScfResult."""
-    X = _orthogonalizer(S)
+            use_diis=True, D0=None, lindep=None):
+    """Restricted Hartree-Fock; build_fock(H, D) -> F.  Returns ScfResult.
+    lindep: optional canonical-orthogonalisation threshold (see _orthogonalizer)."""
+    X = _orthogonalizer(S, lindep)
     if D0 is None:
         _, Cp = np.linalg.eigh(X.T @ H @ X)
         C = X @ Cp
