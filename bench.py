@@ -31,7 +31,7 @@ METRIC = "Fock J/K builds/s + gradient evals/s, mixed vs FP64 at ≤1 µHa / ≤
 UNIT = "steps/s (1 J/K build + 1 gradient eval)"
 WORKLOAD = "c2"
 L2_FLUSH_BYTES = 256 << 20
-MIXED_CUTOFF = 1e-2          # Schwarz x density bound below which quartets run in FP32
+MIXED_CUTOFF = 1e-3          # Schwarz x density bound below which quartets run in FP32
 BATCH_SIZE = 64              # geometries of the batched measurement (8-48 atoms, H-Cl, 6-31G*)
 
 

@@ -33,9 +33,14 @@ def _orthogonalizer(S, lindep=None):
 
 
 def rhf_scf(S, H, e_nuc, n_occ, build_fock, e_tol=1e-10, d_tol=1e-8, max_iter=100, diis_size=8,
-            use_diis=True, D0=None, lindep=None):
+            use_diis=True, D0=None, lindep=None, level_shift=0.0):
     """Restricted Hartree-Fock; build_fock(H, D) -> F.  Returns ScfResult.
-    lindep: optional canonical-orthogonalisation threshold (see _orthogonalizer)."""
+    lindep: optional canonical-orthogonalisation threshold (see _orthogonalizer).
+    level_shift: optional shift (Ha) of the virtual space of the current
+    density before each diagonalisation, F' + shift (1 - P) with P the
+    occupied projector in the orthogonal basis; it damps occupied-virtual
+    oscillations of small-gap systems and leaves the converged solution
+    unchanged (off by default, as in the reference)."""
     X = _orthogonalizer(S, lindep)
     if D0 is None:
         _, Cp = np.linalg.eigh(X.T @ H @ X)
@@ -73,7 +78,11 @@ def rhf_scf(S, H, e_nuc, n_occ, build_fock, e_tol=1e-10, d_tol=1e-8, max_iter=10
                     Fd = sum(ci * fi for ci, fi in zip(c, focks))
                 except np.linalg.LinAlgError:
                     Fd = F
-        eps, Cp = np.linalg.eigh(X.T @ Fd @ X)
+        Fo = X.T @ Fd @ X
+        if level_shift:
+            P = 0.5 * (X.T @ S @ D @ S @ X)
+            Fo = Fo + level_shift * (np.eye(Fo.shape[0]) - P)
+        eps, Cp = np.linalg.eigh(Fo)
         C = X @ Cp
         D = 2.0 * C[:, :n_occ] @ C[:, :n_occ].T
         F = build_fock(H, D)

@@ -25,9 +25,10 @@ def c5():
         S, T, V = eng.one_electron()
         H = T + V
         # S has eigenvalues down to ~2e-8 (diffuse shells on 100 atoms): canonical
-        # orthogonalisation drops those directions, as quantum-chemistry codes do
+        # orthogonalisation drops those directions, as quantum-chemistry codes do;
+        # a 0.2 Ha virtual-level shift steadies the small-gap iterations
         res = rhf_scf(S, H, b.nuclear_repulsion(), b.n_electrons // 2, eng.build_fock, e_tol=1e-9, d_tol=1e-7,
-                      lindep=1e-6)
+                      lindep=1e-6, level_shift=0.2, max_iter=200)
     assert res.converged
     return atoms, basis, b, H, res.density
 
@@ -61,7 +62,7 @@ def test_mixed_bounds_large(c5):
     with FockEngine(b) as eng:
         F0 = eng.build_fock(H, D)
         g0 = eng.eri_gradient(D, 1.0)
-        eng.set_precision(MIXED, 1e-2)
+        eng.set_precision(MIXED, 1e-3)
         eng.autotune(torch.from_numpy(D).cuda().data_ptr(), 1)
         F1 = eng.build_fock(H, D)
         g1 = eng.eri_gradient(D, 1.0)

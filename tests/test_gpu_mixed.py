@@ -17,7 +17,7 @@ from iqcp_b200.molecules import REFERENCE_MOLECULES, workload
 from iqcp_b200.scf import rhf_scf
 
 pytestmark = pytest.mark.gpu
-PRODUCTION_CUTOFF = 1e-2
+PRODUCTION_CUTOFF = 1e-3
 
 
 @pytest.fixture(scope="module")
