@@ -133,7 +133,7 @@ class BatchRHF:
     """Device-resident batched RHF over the geometries of a BatchFockEngine."""
 
     def __init__(self, bases, n_groups=8, purify_iters=64, precision=FP64, mixed_cutoff=1e-9, device=0,
-                 engine=None):
+                 engine=None, level_shift=0.0):
         self.dev = torch.device("cuda", device)
         self.eng = engine if engine is not None else BatchFockEngine(bases, precision=precision,
                                                                     mixed_cutoff=mixed_cutoff, device=device)
@@ -142,6 +142,10 @@ class BatchRHF:
         if any(b.n_electrons % 2 for b in self.bases):
             raise ValueError("closed-shell geometries only")
         self.purify_iters = purify_iters
+        # virtual-level shift (Ha) of the extrapolated Fock matrix: F' + s (1 - P),
+        # P the occupied projector of the current density; damps occupied-virtual
+        # oscillations of small-gap geometries, converged solution unchanged
+        self.level_shift = float(level_shift)
         S, T, V = (torch.from_numpy(x).to(self.dev) for x in self._one_electron_packed())
         self.H_p = T + V
         self.D_p = torch.zeros_like(S)
@@ -215,6 +219,11 @@ class BatchRHF:
             c = c / c.sum(dim=1, keepdim=True)
             Fx = torch.einsum("bk,kbij->bij", c, g.Fbuf)
             Fp = g.X.transpose(1, 2) @ Fx @ g.X
+            if self.level_shift:
+                XS = g.X.transpose(1, 2) @ g.S
+                Pocc = 0.5 * (XS @ D @ XS.transpose(1, 2))
+                eye_n = torch.eye(g.n, dtype=Fp.dtype, device=self.dev)
+                Fp = Fp + self.level_shift * (eye_n - Pocc)
             # padding levels at the top of the spectrum, above every real level
             top = Fp.abs().sum(dim=2).amax(dim=1) + 1.0
             real = (~g.pad[:, :, None] & ~g.pad[:, None, :]).to(Fp.dtype)
