@@ -118,7 +118,12 @@ int iqcp_nbf(const iqcp_ctx* ctx);
  */
 int iqcp_set_precision(iqcp_ctx* ctx, int precision, double mixed_cutoff);
 
-/* Run the context's work on this CUDA stream (cudaStream_t); NULL = its own stream. */
+/*
+ * Run the context's work on this CUDA stream (cudaStream_t); NULL = the
+ * context's own stream, which is created non-blocking (it does not order with
+ * the legacy default stream).  A caller working on the legacy default stream
+ * passes cudaStreamLegacy, not NULL.
+ */
 int iqcp_set_stream(iqcp_ctx* ctx, void* stream);
 
 /*

@@ -29,6 +29,7 @@ __all__ = ["BasisSet", "FockEngine", "IqcpError", "boys_eval_all", "rys_roots", 
 
 ANGSTROM_TO_BOHR = 1.8897261245650618  # constants.rs:63
 FP64, MIXED = 0, 1
+_CUDA_STREAM_LEGACY = 0x1   # cudaStreamLegacy
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = None
@@ -382,7 +383,13 @@ class FockEngine:
         self._check(self._lib.iqcp_set_precision(self._h, int(precision), float(mixed_cutoff)))
 
     def set_stream(self, stream_handle):
-        self._check(self._lib.iqcp_set_stream(self._h, ctypes.c_void_p(stream_handle)))
+        """Enqueue the device forms on this CUDA stream (e.g. torch's
+        current_stream().cuda_stream).  Handle 0, torch's default stream, is
+        the legacy default stream: it is passed as cudaStreamLegacy, since a
+        NULL stream selects the context's own non-blocking stream, which would
+        not order with work on the default stream."""
+        h = int(stream_handle or 0)
+        self._check(self._lib.iqcp_set_stream(self._h, ctypes.c_void_p(h if h else _CUDA_STREAM_LEGACY)))
 
 
 class BatchFockEngine(FockEngine):

@@ -133,7 +133,10 @@ class BatchRHF:
     """Device-resident batched RHF over the geometries of a BatchFockEngine."""
 
     def __init__(self, bases, n_groups=8, purify_iters=64, precision=FP64, mixed_cutoff=1e-9, device=0,
-                 engine=None, level_shift=0.0):
+                 engine=None, level_shift=0.0, D0=None):
+        """D0: optional list of starting densities (default: core-Hamiltonian guess)."""
+        self._opts = dict(purify_iters=purify_iters, precision=precision, mixed_cutoff=mixed_cutoff,
+                          device=device, level_shift=level_shift)
         self.dev = torch.device("cuda", device)
         self.eng = engine if engine is not None else BatchFockEngine(bases, precision=precision,
                                                                     mixed_cutoff=mixed_cutoff, device=device)
@@ -165,12 +168,15 @@ class BatchRHF:
             if float(w.min()) <= 1e-10:
                 raise ValueError("overlap matrix is singular")
             g.X = (U / torch.sqrt(w)[:, None, :]) @ U.transpose(1, 2)
-            # core-Hamiltonian guess (scf/mod.rs:1379-1389), eagerly, before capture
-            Hp = g.X.transpose(1, 2) @ g.H @ g.X + torch.diag_embed(g.pad.to(torch.float64) * 1e6)
-            _, C = torch.linalg.eigh(Hp)
-            Cx = g.X @ C
-            occ = (torch.arange(g.n, device=self.dev)[None, :] < g.nocc[:, None]).to(torch.float64)
-            g.D = (2.0 * (Cx * occ[:, None, :]) @ Cx.transpose(1, 2)) * g.valid
+            if D0 is None:
+                # core-Hamiltonian guess (scf/mod.rs:1379-1389), eagerly, before capture
+                Hp = g.X.transpose(1, 2) @ g.H @ g.X + torch.diag_embed(g.pad.to(torch.float64) * 1e6)
+                _, C = torch.linalg.eigh(Hp)
+                Cx = g.X @ C
+                occ = (torch.arange(g.n, device=self.dev)[None, :] < g.nocc[:, None]).to(torch.float64)
+                g.D = (2.0 * (Cx * occ[:, None, :]) @ Cx.transpose(1, 2)) * g.valid
+            else:
+                g.D = g.unpack(torch.from_numpy(eng.pack(D0)).to(self.dev))
             g.pack_into(self.D_p, g.D)
             B = len(g.mols)
             g.Fbuf = torch.zeros((DIIS_SIZE, B, g.n, g.n), dtype=torch.float64, device=self.dev)
@@ -254,12 +260,39 @@ class BatchRHF:
         self.graph = g
         return g
 
-    def run(self, e_tol=1e-9, d_tol=1e-7, err_tol=1e-5, max_iter=80, use_graph=True):
+    def _gather(self, name):
+        order = np.concatenate([g.mols for g in self.groups])
+        v = np.empty(len(self.bases))
+        v[order] = torch.cat([getattr(g, name) for g in self.groups]).cpu().numpy()
+        return v
+
+    def _set_density(self, m, D):
+        """Overwrite geometry m's density (packed array and its group's block)."""
+        lo, hi = int(self.eng.mat_offset[m]), int(self.eng.mat_offset[m + 1])
+        Dt = torch.from_numpy(np.ascontiguousarray(D)).to(self.dev)
+        self.D_p[lo:hi] = Dt.reshape(-1)
+        for g in self.groups:
+            k = np.flatnonzero(g.mols == m)
+            if len(k):
+                n = D.shape[0]
+                g.D[int(k[0]), :n, :n] = Dt
+
+    def run(self, e_tol=1e-9, d_tol=1e-7, err_tol=1e-5, max_iter=80, use_graph=True, handoff=None,
+            handoff_after=10):
+        """Iterate until every geometry meets the three thresholds or max_iter.
+
+        handoff: optional fraction; once at least that share of the geometries
+        has converged (after handoff_after iterations), the others continue in a
+        new batched context of their own, seeded with their current densities
+        (DIIS restarts), so the converged ones stop costing Fock builds.  Their
+        results and densities are written back, so gradients() still covers the
+        whole batch."""
         if use_graph and self.graph is None:
             self.capture()
         self.eng.set_stream(torch.cuda.current_stream(self.dev).cuda_stream)
         it = 0
-        conv = None
+        order = np.concatenate([g.mols for g in self.groups])
+        conv = np.zeros(len(self.bases), bool)
         for it in range(1, max_iter + 1):
             if use_graph:
                 self.graph.replay()
@@ -268,18 +301,32 @@ class BatchRHF:
             stats = torch.stack([torch.cat([g.dE.abs() for g in self.groups]),
                                  torch.cat([g.dD for g in self.groups]),
                                  torch.cat([g.err for g in self.groups])]).cpu().numpy()
-            conv = (stats[0] < e_tol) & (stats[1] < d_tol) & (stats[2] < err_tol)
+            conv = np.empty(len(self.bases), bool)
+            conv[order] = (stats[0] < e_tol) & (stats[1] < d_tol) & (stats[2] < err_tol)
             if it > 2 and conv.all():
                 break
-        order = np.concatenate([g.mols for g in self.groups])
-        out = {}
-        for name in ("E", "idem"):
-            v = np.empty(len(self.bases))
-            v[order] = torch.cat([getattr(g, name) for g in self.groups]).cpu().numpy()
-            out[name] = v
-        converged = np.empty(len(self.bases), bool)
-        converged[order] = conv
-        return BatchScfResult(energies=out["E"], converged=converged, iterations=it, idempotency=out["idem"])
+            if (handoff is not None and it >= handoff_after and it < max_iter and conv.mean() >= handoff
+                    and len(self.bases) > 1):
+                break
+        energies, idem = self._gather("E"), self._gather("idem")
+        iterations = it
+        pending = np.flatnonzero(~conv)
+        if handoff is not None and len(pending) and it < max_iter and len(pending) < len(self.bases):
+            dens = self.densities()
+            sub = BatchRHF([self.bases[i] for i in pending], n_groups=min(len(pending), 8),
+                           D0=[dens[i] for i in pending], **self._opts)
+            sub.eng.set_stream(torch.cuda.current_stream(self.dev).cuda_stream)
+            sub.eng.autotune(sub.D_p.data_ptr(), 1)
+            r = sub.run(e_tol=e_tol, d_tol=d_tol, err_tol=err_tol, max_iter=max_iter - it, use_graph=use_graph)
+            for j, i in enumerate(pending):
+                energies[i], idem[i], conv[i] = r.energies[j], r.idempotency[j], r.converged[j]
+            for j, D in enumerate(sub.densities()):
+                self._set_density(int(pending[j]), D)
+            iterations = it + r.iterations
+            sub.graph = None
+            sub.eng.close()
+            self.eng.set_stream(torch.cuda.current_stream(self.dev).cuda_stream)
+        return BatchScfResult(energies=energies, converged=conv, iterations=iterations, idempotency=idem)
 
     def densities(self):
         return self.eng.unpack(self.D_p.cpu().numpy())

@@ -47,3 +47,23 @@ def test_batch_rhf_energies_and_gradients(bases, reference, use_graph):
         assert abs(e - e_ref) < 1e-8, (e, e_ref)
         assert np.abs(d - d_ref).max() < 1e-5
         assert np.abs(g - g_ref).max() < 1e-6
+
+
+def test_batch_rhf_handoff(bases, reference):
+    """Hand-off of the unconverged geometries to a smaller batch after a few
+    iterations reaches the same energies, densities and gradients."""
+    from iqcp_b200.batch_scf import BatchRHF
+
+    scf = BatchRHF(bases, n_groups=3)
+    res = scf.run(e_tol=1e-10, d_tol=1e-8, err_tol=1e-7, handoff=0.3, handoff_after=3)
+    assert res.converged.all(), res.__dict__
+    grads = scf.gradients()
+    # the device calls and the torch steps between them share one stream: a
+    # second evaluation agrees to rounding
+    again = scf.gradients()
+    assert max(np.abs(a - b).max() for a, b in zip(grads, again)) < 1e-10
+    dens = scf.densities()
+    for (e_ref, g_ref, d_ref), e, g, d in zip(reference, res.energies, grads, dens):
+        assert abs(e - e_ref) < 1e-8, (e, e_ref)
+        assert np.abs(d - d_ref).max() < 1e-5
+        assert np.abs(g - g_ref).max() < 1e-6

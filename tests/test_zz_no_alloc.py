@@ -25,6 +25,7 @@ def _run(eng, torch, D, noalloc):
     dK = torch.empty_like(dD)
     lib = eng._lib
     fn = lib.iqcp_jk_device_noalloc if noalloc else lib.iqcp_jk_device
+    torch.cuda.synchronize()  # the input copy is on torch's stream, the build on the context's own
     rc = fn(eng._h, ctypes.c_void_p(dD.data_ptr()), ctypes.c_void_p(dJ.data_ptr()), ctypes.c_void_p(dK.data_ptr()))
     assert rc == 0, lib.iqcp_last_error(eng._h).decode()
     torch.cuda.synchronize()
