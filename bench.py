@@ -55,6 +55,24 @@ def parse():
     return ap.parse_args()
 
 
+def max_over_ranks(x, world):
+    """Largest value of x over the ranks (every rank calls this, in the same
+    order); the job's time is the slowest replica's."""
+    if world <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(world, steps, seconds):
+    """Whole-job steps/s: each of `world` replicas runs `steps` steps in at most `seconds`."""
+    return world * steps / seconds
+
+
 def workload_config(b, seed):
     return {"workload": "40-atom C/N/O/H molecule, RHF/6-31G* (%d Cartesian bf, %d shells), seed %d"
                         % (b.n_basis, b.n_shells, seed),
@@ -155,8 +173,6 @@ def measure_mixed(args, eng, b, H, D, dD, dJ, dK, dg, flush, stream, world):
     """The mixed form at MIXED_CUTOFF: FP32 quadrature for quartets whose
     Schwarz x density bound is below it (autotuned split per class), timed like
     the FP64 step, with its energy, Fock and gradient errors against FP64."""
-    import torch
-    import torch.distributed as dist
     from iqcp_b200 import FP64, MIXED
     F64 = eng.build_fock(H, D)
     g64 = eng.eri_gradient(D, 1.0)
@@ -171,11 +187,7 @@ def measure_mixed(args, eng, b, H, D, dD, dJ, dK, dg, flush, stream, world):
 
     for _ in range(args.warmup):
         step()
-    t_ms = timed_steps(step, args.steps, flush, stream)
-    if world > 1:
-        tt = torch.tensor([t_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_ms = float(tt.item())
+    t_ms = max_over_ranks(timed_steps(step, args.steps, flush, stream), world)
     eng.jk_device(dD.data_ptr(), dJ.data_ptr(), dK.data_ptr())
     nq = eng.last_stats()
     eng.eri_gradient_device(dD.data_ptr(), 1.0, dg.data_ptr())
@@ -186,7 +198,7 @@ def measure_mixed(args, eng, b, H, D, dD, dJ, dK, dg, flush, stream, world):
     modes = eng.kernel_modes()
     eng.set_precision(FP64)
     de, dgmax = abs(e - e64), float(np.abs(g - g64).max())
-    return {"cutoff": MIXED_CUTOFF, "value": world * args.steps / (t_ms * 1e-3), "unit": UNIT,
+    return {"cutoff": MIXED_CUTOFF, "value": job_throughput(world, args.steps, t_ms * 1e-3), "unit": UNIT,
             "ms_per_step": t_ms / args.steps,
             "energy_error_ha": de, "fock_max_error_ha": float(np.abs(F - F64).max()),
             "grad_max_error_ha_bohr": dgmax, "within_bounds": bool(de <= 1e-6 and dgmax <= 1e-6),
@@ -377,14 +389,11 @@ def main():
         torch.cuda.synchronize()
     torch.cuda.nvtx.range_pop()
     eng.set_profiling(False)
-    t_ms = sum(a.elapsed_time(b_) for a, b_ in ev)
+    t_ms = max_over_ranks(sum(a.elapsed_time(b_) for a, b_ in ev), world)
     if world > 1:
-        tt = torch.tensor([t_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_ms = float(tt.item())
         dist.barrier()
     clocks = clk.summary()
-    value = world * args.steps / (t_ms * 1e-3)
+    value = job_throughput(world, args.steps, t_ms * 1e-3)
 
     # end to end through the public host-buffer API (pinned host memory)
     hD = torch.from_numpy(D).pin_memory().numpy()
@@ -398,11 +407,8 @@ def main():
         J, K = eng.build_jk(hD)
         g = eng.eri_gradient(hD, 1.0)
         e2e_t += time.perf_counter() - t0
-    if world > 1:
-        tt = torch.tensor([e2e_t], dtype=torch.float64, device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_t = float(tt.item())
-    e2e = {"value": world * args.steps / e2e_t, "unit": UNIT,
+    e2e_t = max_over_ranks(e2e_t, world)
+    e2e = {"value": job_throughput(world, args.steps, e2e_t), "unit": UNIT,
            "h2d_bytes_per_step": 2 * n * n * 8 + b.n_atoms * 3 * 8,
            "d2h_bytes_per_step": 2 * n * n * 8 + b.n_atoms * 3 * 8}
 
