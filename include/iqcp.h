@@ -143,6 +143,9 @@ int iqcp_fock(iqcp_ctx* ctx, const double* H, const double* D, double k_scale, d
 
 /*
  * Device-pointer forms of iqcp_jk / iqcp_fock for data resident in HBM.  They
+ * enqueue their kernels on the context stream (iqcp_set_stream) and may return
+ * before the outputs are written: order with them on that stream, or
+ * synchronise it, before reading the outputs from another stream.  They
  * (and iqcp_eri_grad_device, iqcp_one_electron_grad_device) may be captured
  * into a CUDA graph on the context stream (iqcp_set_stream to the capturing
  * stream): while the stream captures they only enqueue work, and
