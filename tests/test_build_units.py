@@ -1,0 +1,23 @@
+"""The committed kernel instantiation units are exactly what gen_inst.py
+writes (one per kernel kind, quadrature type, bra class and ket class, plus a
+dispatch unit per kind and bra class), so the build and its generator agree."""
+import glob
+import os
+import shutil
+import subprocess
+import sys
+
+CSRC = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "iqcp_b200", "csrc")
+
+
+def test_instantiation_units_match_generator(tmp_path):
+    shutil.copy(os.path.join(CSRC, "gen_inst.py"), tmp_path)
+    subprocess.run([sys.executable, "gen_inst.py"], cwd=tmp_path, check=True)
+    made = sorted(os.path.basename(f) for f in glob.glob(str(tmp_path / "eri_inst_*.cu")))
+    have = sorted(os.path.basename(f) for f in glob.glob(os.path.join(CSRC, "eri_inst_*.cu")))
+    assert made == have
+    for name in made:
+        with open(tmp_path / name) as a, open(os.path.join(CSRC, name)) as b:
+            assert a.read() == b.read(), name
+    # 21 class pairs x 2 kinds x 2 precisions + 6 dispatch x 2 kinds + 6 store units
+    assert len(made) == 21 * 4 + 12 + 6
