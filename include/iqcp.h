@@ -158,16 +158,20 @@ int iqcp_fock_device(iqcp_ctx* ctx, const double* d_H, const double* d_D, double
 
 /*
  * iqcp_jk_device without any device allocation: same inputs, outputs and
- * results, but its scratch (scaled density, J/K accumulators) lives in a
+ * results as iqcp_jk_device in either precision (FP64 or MIXED, as set on the
+ * context), but its scratch (scaled density, J/K accumulators) lives in a
  * fixed file-scope device array instead of context buffers.  No counterpart
  * in the reference.  For callers whose Fock-build loop may not call cudaMalloc
  * (all of HBM handed to their own pool, or no implicit device synchronisation
  * allowed); the context is created beforehand by iqcp_create.
  * Limit: nbf <= 512 (3*512*512 doubles, 6 MiB held on every GPU that loads the
- * library); larger bases return IQCP_ERR_ARG.  The first call on a device
- * looks up the array's address (cudaGetSymbolAddress) -- make it before any
- * stream capture.  All calls share the array: calls that overlap on the GPU
- * race, so serialise them.
+ * library); larger bases and batched contexts return IQCP_ERR_ARG.  The first
+ * call on a device looks up the array's address (cudaGetSymbolAddress) --
+ * make it before any stream capture.  The call enqueues its work on the
+ * context stream and returns without waiting for the GPU; iqcp_last_stats
+ * then reports quartets and launches but 0 for device time and FP32 count.
+ * All calls share the array: calls that overlap on the GPU race, so
+ * serialise them.
  */
 int iqcp_jk_device_noalloc(iqcp_ctx* ctx, const double* d_D, double* d_J, double* d_K);
 

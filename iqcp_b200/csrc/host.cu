@@ -749,8 +749,8 @@ int iqcp_fock_device(iqcp_ctx* ctx, const double* dH, const double* dD, double k
 // entry point keeps its scratch -- the angular-scaled density and the two
 // unsymmetrised J/K accumulators -- in one file-scope device array of fixed
 // size instead of the context's own buffers.  The context itself (pair tables,
-// quartet lists) is built beforehand by iqcp_create, where allocation is
-// allowed.
+// quartet lists, the mixed form's density-bound table and masks) is built
+// beforehand by iqcp_create, where allocation is allowed.
 //
 // Limits and rules:
 //   * nbf <= IQCP_NOALLOC_MAX_NBF (512): the array holds 3 * 512 * 512 doubles
@@ -763,6 +763,9 @@ int iqcp_fock_device(iqcp_ctx* ctx, const double* dH, const double* dD, double k
 //     the accumulators are cleared at the start of every call.  Calls whose
 //     work overlaps on the GPU (other streams, other host threads) race on the
 //     array: serialise them.
+//   * The call only enqueues work on the context stream and returns without
+//     waiting for the GPU; iqcp_last_stats reports its screened quartets and
+//     launches, not its device time or FP32 count (both 0).
 #define IQCP_NOALLOC_MAX_NBF 512
 static __device__ __align__(256) double g_noalloc_scratch[3 * IQCP_NOALLOC_MAX_NBF * IQCP_NOALLOC_MAX_NBF];
 static double* g_noalloc_ptr[64] = {nullptr};
@@ -798,18 +801,29 @@ int iqcp_jk_device_noalloc(iqcp_ctx* ctx, const double* dD, double* dJ, double* 
   double* Jt = scratch + nn;
   double* Kt = scratch + 2 * nn;
   const bool want_k = dK != nullptr;
-  const bool prof = ctx->profile;
-  ctx->profile = false;  // per-launch timing would create events
-  ctx->mixed_call = false;
+  // per-launch timing would create events: off for this call, restored on every exit
+  struct ProfileOff {
+    iqcp_ctx* c;
+    bool saved;
+    ~ProfileOff() { c->profile = saved; }
+  } guard{ctx, ctx->profile};
+  ctx->profile = false;
+  ctx->stats[2] = ctx->stats[3] = 0.0;
   ctx->launches_total = 1;
   CK(launch_scale_density(dD, ctx->d_ang, ctx->pack, Ds, ctx->stream));
+  // the mixed form uses only context buffers (density bounds, task masks)
+  ctx->mixed_call = ctx->opt.precision == IQCP_MIXED;
+  if (ctx->mixed_call) {
+    rc = prepare_mixed(ctx, dD, 0);
+    if (rc) return rc;
+  }
   CK(cudaMemsetAsync(Jt, 0, sizeof(double) * nn, ctx->stream));
   if (want_k) CK(cudaMemsetAsync(Kt, 0, sizeof(double) * nn, ctx->stream));
   rc = run_ranges(ctx, 0, [&](const TaskRange& r, int pass, int* counter) {
-    const JKArgs a = jk_args(ctx, r, Ds, Jt, want_k ? Kt : nullptr, r.mode[0], pass, counter);  // FP64 only
+    const JKArgs a = jk_args(ctx, r, Ds, Jt, want_k ? Kt : nullptr, pass == 2 ? r.mode32[0] : r.mode[0], pass,
+                             counter);
     return launch_jk(r.X, r.Y, a, ctx->stream);
   });
-  ctx->profile = prof;
   if (rc) return rc;
   CK(launch_symmetrize(Jt, ctx->d_ang, ctx->pack, dJ, ctx->stream));
   ctx->launches_total += 1;
@@ -817,11 +831,7 @@ int iqcp_jk_device_noalloc(iqcp_ctx* ctx, const double* dD, double* dJ, double* 
     CK(launch_symmetrize(Kt, ctx->d_ang, ctx->pack, dK, ctx->stream));
     ctx->launches_total += 1;
   }
-  float ms = 0.f;
-  CK(cudaEventSynchronize(ctx->ev1));
-  CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
-  ctx->stats[2] = ms * 1e3;
-  return IQCP_OK;
+  return IQCP_OK;  // enqueued only: no wait for the GPU
 }
 
 int iqcp_jk(iqcp_ctx* ctx, const double* D, double* J, double* K) {
