@@ -3,15 +3,19 @@
 
 One step = one direct J/K build plus one two-electron gradient evaluation on
 the same density, for the 40-atom RHF/6-31G* workload (392 Cartesian basis
-functions, d shells up to (dd|dd) at Rys order 5; seeded synthetic molecule,
-converged RHF density from an SCF run with this library before timing).
+functions, d shells up to (dd|dd) at Rys order 5; seeded synthetic molecule).
+The density is the oracle-converged RHF density committed in
+tests/golden/config_c2.npz (the reference algorithm's own SCF solution), so
+both arms and the parity figures use the same input.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl iqcp|reference]
 
 Under torchrun every rank runs an independent replica on its own GPU (the
 path has no exchange step); rank 0 prints one JSON line.  ``--impl reference``
 times the reference algorithm's CPU restatement (the oracle; the reference's
-Rust code cannot be built here) on a bounded sample of the same workload.
+Rust code cannot be built here) without loading the product library: the K
+timed steps evaluate every K-th bra shell pair at phases 0..K-1, so together
+they are exactly one full J/K build and one full gradient.
 """
 import argparse
 import json
@@ -32,7 +36,8 @@ UNIT = "steps/s (1 J/K build + 1 gradient eval)"
 WORKLOAD = "c2"
 L2_FLUSH_BYTES = 256 << 20
 MIXED_CUTOFF = 1e-3          # Schwarz x density bound below which quartets run in FP32
-BATCH_SIZE = 64              # geometries of the batched measurement (8-48 atoms, H-Cl, 6-31G*)
+BATCH_SIZE = 256             # geometries of the batched measurement (8-48 atoms, H-Cl, 6-31G*)
+FIXTURE = os.path.join(ROOT, "tests", "golden", "config_c2.npz")
 
 
 def parse():
@@ -77,9 +82,33 @@ def workload_config(b, seed):
     return {"workload": "40-atom C/N/O/H molecule, RHF/6-31G* (%d Cartesian bf, %d shells), seed %d"
                         % (b.n_basis, b.n_shells, seed),
             "basis": "6-31g*", "n_atoms": int(b.n_atoms), "nbf": int(b.n_basis),
-            "step": "1 direct J/K build + 1 two-electron gradient, converged RHF density",
+            "step": "1 direct J/K build + 1 two-electron gradient, oracle-converged RHF density",
             "screening": "Schwarz 1e-12, primitive K 1e-15",
             "l2": "flushed between timed steps (256 MiB device write)"}
+
+
+def load_fixture():
+    """Geometry, oracle-converged density and the oracle's energy and gradients of
+    the 40-atom workload (tests/golden/config_c2.npz, written by
+    tests/golden/make_config_fixtures.py)."""
+    f = np.load(FIXTURE)
+    meta = json.loads(str(f["meta"]))
+    atoms = [(int(z), tuple(float(v) for v in x)) for z, x in zip(f["z"], f["xyz"])]
+    C = f["c_occ"]
+    return {"atoms": atoms, "basis": meta["basis"], "meta": meta, "D": 2.0 * C @ C.T, "c_occ": C,
+            "eps_occ": f["eps_occ"], "grad_2e": f["grad_2e"], "grad_rhf": f["grad_rhf"], "energy": meta["energy"]}
+
+
+def oracle_sample(b, D, stride, phase):
+    """Wall time of the oracle's J/K and gradient over the bra shell pairs P with
+    P % stride == phase (all host threads)."""
+    import oracle
+    t0 = time.perf_counter()
+    oracle.jk_direct(b, D, stride, phase)
+    t1 = time.perf_counter()
+    oracle.eri_gradient(b, D, 1.0, stride, phase)
+    t2 = time.perf_counter()
+    return t1 - t0, t2 - t1
 
 
 def cpu_baseline(b, D, stride, phase=0):
@@ -87,16 +116,49 @@ def cpu_baseline(b, D, stride, phase=0):
     shell pair, all host threads; scaled to the full workload."""
     import oracle
     threads = oracle.max_threads()
-    t0 = time.perf_counter()
-    _, _, cnt = oracle.jk_direct(b, D, stride, phase)
-    t1 = time.perf_counter()
-    oracle.eri_gradient(b, D, 1.0, stride, phase)
-    t2 = time.perf_counter()
-    t_step = (t1 - t0) * stride + (t2 - t1) * stride
+    tj, tg = oracle_sample(b, D, stride, phase)
+    t_step = (tj + tg) * stride
     return {"value": 1.0 / t_step, "unit": UNIT, "cores": threads, "kind": "port",
             "sample": "every %d-th bra shell pair of the same workload (J/K %.1f s + gradient %.1f s of CPU "
-                      "wall time, scaled by %d)" % (stride, t1 - t0, t2 - t1, stride),
-            "jk_s": (t1 - t0) * stride, "grad_s": (t2 - t1) * stride}
+                      "wall time, scaled by %d)" % (stride, tj, tg, stride),
+            "jk_s": tj * stride, "grad_s": tg * stride}
+
+
+def single_thread_fock(eng_cls, basis_cls):
+    """The reference's published single-thread figure is its stored-ERI Fock
+    build inside the C6H6 RHF/6-31G* SCF (102 bf; 2380.7 ms for 13 builds on a
+    Ryzen 7 5800X, results_native.json:957).  The oracle's stored build_fock
+    (the same algorithm) on one host thread, and the device build, on that
+    molecule."""
+    import oracle
+    from oracle.basis import build_basis
+    from iqcp_b200.molecules import REFERENCE_MOLECULES
+    atoms = REFERENCE_MOLECULES["C6H6"]
+    ob = build_basis(atoms, "6-31g*")
+    eri, _ = oracle.eri_compressed(ob)      # untimed, all threads
+    H = oracle.hcore(ob)
+    rng = np.random.default_rng(1)
+    A = rng.normal(size=(ob.n_basis, ob.n_basis)) * 0.05
+    D = A + A.T
+    threads = oracle.max_threads()
+    oracle.set_threads(1)
+    try:
+        oracle.build_fock(H, D, eri)
+        t0 = time.perf_counter()
+        for _ in range(3):
+            oracle.build_fock(H, D, eri)
+        t_cpu = (time.perf_counter() - t0) / 3
+    finally:
+        oracle.set_threads(threads)
+    with eng_cls(basis_cls.build(atoms, "6-31g*")) as eng:
+        eng.build_fock(H, D)
+        t0 = time.perf_counter()
+        for _ in range(10):
+            eng.build_fock(H, D)
+        t_gpu = (time.perf_counter() - t0) / 10
+    return {"workload": "C6H6 RHF/6-31G* (102 bf), one Fock build", "oracle_1thread_ms": t_cpu * 1e3,
+            "published_reference_ms": 2380.7 / 13, "published_hardware": "Ryzen 7 5800X, 1 thread (stored ERIs)",
+            "device_e2e_ms": t_gpu * 1e3}
 
 
 class ClockSampler:
@@ -169,14 +231,16 @@ def timed_steps(step, steps, flush, stream):
     return sum(a.elapsed_time(b_) for a, b_ in ev)
 
 
-def measure_mixed(args, eng, b, H, D, dD, dJ, dK, dg, flush, stream, world):
+def measure_mixed(args, eng, b, H, S, fx, dD, dJ, dK, dg, flush, stream, world, fp64):
     """The mixed form at MIXED_CUTOFF: FP32 quadrature for quartets whose
     Schwarz x density bound is below it (autotuned split per class), timed like
-    the FP64 step, with its energy, Fock and gradient errors against FP64."""
+    the FP64 step.  Errors against the oracle: the converged SCF energy (SCF
+    driven by mixed Fock builds, started from the oracle's density) against the
+    oracle's converged energy, and the two-electron gradient at the oracle's
+    density against the oracle's; also against the device FP64 form."""
     from iqcp_b200 import FP64, MIXED
-    F64 = eng.build_fock(H, D)
-    g64 = eng.eri_gradient(D, 1.0)
-    e64 = 0.5 * float(np.sum(D * (H + F64)))
+    from iqcp_b200.scf import rhf_scf
+    D = fx["D"]
     eng.set_precision(MIXED, MIXED_CUTOFF)
     eng.autotune(dD.data_ptr(), 2)
 
@@ -194,57 +258,80 @@ def measure_mixed(args, eng, b, H, D, dD, dJ, dK, dg, flush, stream, world):
     ng = eng.last_stats()
     F = eng.build_fock(H, D)
     g = eng.eri_gradient(D, 1.0)
-    e = 0.5 * float(np.sum(D * (H + F)))
+    scf = rhf_scf(S, H, b.nuclear_repulsion(), b.n_electrons // 2, eng.build_fock, e_tol=1e-10, d_tol=1e-8, D0=D)
     modes = eng.kernel_modes()
     eng.set_precision(FP64)
-    de, dgmax = abs(e - e64), float(np.abs(g - g64).max())
+    e_at_d = 0.5 * float(np.sum(D * (H + F)))
+    de_scf = abs(scf.energy - fx["energy"])
+    dg_oracle = float(np.abs(g - fx["grad_2e"]).max())
     return {"cutoff": MIXED_CUTOFF, "value": job_throughput(world, args.steps, t_ms * 1e-3), "unit": UNIT,
-            "ms_per_step": t_ms / args.steps,
-            "energy_error_ha": de, "fock_max_error_ha": float(np.abs(F - F64).max()),
-            "grad_max_error_ha_bohr": dgmax, "within_bounds": bool(de <= 1e-6 and dgmax <= 1e-6),
+            "ms_per_step": t_ms / args.steps, "speedup_vs_fp64": fp64["ms_per_step"] / (t_ms / args.steps),
+            "energy_error_vs_oracle_ha": de_scf, "scf_energy": scf.energy, "scf_iterations": scf.iterations,
+            "grad_error_vs_oracle_ha_bohr": dg_oracle,
+            "energy_error_vs_fp64_at_density_ha": abs(e_at_d - fp64["e_at_d"]),
+            "fock_max_error_vs_fp64_ha": float(np.abs(F - fp64["F"]).max()),
+            "grad_max_error_vs_fp64_ha_bohr": float(np.abs(g - fp64["g"]).max()),
+            "within_bounds": bool(de_scf <= 1e-6 and dg_oracle <= 1e-6),
             "fp32_quartet_share_jk": nq["fp32_quartets"] / max(nq["quartets"], 1),
             "fp32_quartet_share_grad": ng["fp32_quartets"] / max(ng["quartets"], 1),
             "split_classes": {"jk": int(((modes[2] >= 0) & (modes[2] < 4)).sum()),
                               "grad": int(((modes[3] >= 0) & (modes[3] < 4)).sum()), "of": 21},
             "note": "FP32 quadrature (FP64 roots, weights, accumulation) for quartets with "
                     "Q_ij Q_kl max|D| (gradient: max|D|^2) below the cutoff, in the classes where the autotuner "
-                    "found the FP64/FP32 split faster than FP64 alone; errors against the FP64 form at the same "
-                    "density"}
+                    "found the FP64/FP32 split faster than FP64 alone; bars 1e-6 Ha and 1e-6 Ha/bohr against the "
+                    "oracle"}
 
 
 def measure_batch(args):
     """Batched context: BATCH_SIZE seeded geometries of uneven size through one
-    context; one step = one J/K build + one gradient of every geometry."""
+    context; one step = one J/K build + one gradient of every geometry, FP64
+    and mixed (core-Hamiltonian guess densities; the quartet lists, not D,
+    set the cost of the FP64 form)."""
     import torch
-    from iqcp_b200 import BasisSet
+    from iqcp_b200 import FP64, MIXED, BasisSet
     from iqcp_b200.batch_scf import BatchRHF
     from iqcp_b200.molecules import batch_geometries
     t0 = time.perf_counter()
     geoms = batch_geometries(args.batch, seed=args.seed)
     bases = [BasisSet.build(a, "6-31g*") for a in geoms]
-    scf = BatchRHF(bases)          # packed H, core-guess densities, batched context
+    scf = BatchRHF(bases)          # batched context
     eng = scf.eng
     stream = torch.cuda.current_stream()
     eng.set_stream(stream.cuda_stream)
-    eng.autotune(scf.D_p.data_ptr(), 1)
+    Dp = torch.from_numpy(scf.core_guess()).to("cuda")     # core-Hamiltonian guess of every geometry
+    eng.autotune(Dp.data_ptr(), 1)
     setup_s = time.perf_counter() - t0
-    J = torch.empty_like(scf.D_p)
-    K = torch.empty_like(scf.D_p)
+    J = torch.empty_like(Dp)
+    K = torch.empty_like(Dp)
     g = torch.zeros((eng.n_atoms, 3), dtype=torch.float64, device="cuda")
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
 
     def jk():
-        eng.jk_device(scf.D_p.data_ptr(), J.data_ptr(), K.data_ptr())
+        eng.jk_device(Dp.data_ptr(), J.data_ptr(), K.data_ptr())
 
     def grad():
         g.zero_()
-        eng.eri_gradient_device(scf.D_p.data_ptr(), 1.0, g.data_ptr())
+        eng.eri_gradient_device(Dp.data_ptr(), 1.0, g.data_ptr())
 
-    jk()
-    grad()
-    steps = max(1, min(args.steps, 3))
-    tj = timed_steps(jk, steps, flush, stream) / steps
-    tg = timed_steps(grad, steps, flush, stream) / steps
+    def measure():
+        jk()
+        grad()
+        steps = max(1, min(args.steps, 3))
+        tj = timed_steps(jk, steps, flush, stream) / steps
+        tg = timed_steps(grad, steps, flush, stream) / steps
+        jk()
+        grad()
+        torch.cuda.synchronize()
+        return tj, tg, (J - 0.5 * K).clone(), g.clone()
+
+    tj, tg, G64, g64 = measure()
+    eng.set_precision(MIXED, MIXED_CUTOFF)
+    eng.autotune(Dp.data_ptr(), 1)
+    tjm, tgm, G32, g32 = measure()
+    eng.set_precision(FP64)
+    # per-geometry two-electron energy 1/2 Tr D G, mixed against FP64
+    dE = torch.stack([0.5 * torch.sum(Dp[a:b] * (G32[a:b] - G64[a:b]))
+                      for a, b in zip(eng.mat_offset[:-1], eng.mat_offset[1:])]).abs().max().item()
     nbf = np.array([bb.n_basis for bb in bases])
     out = {"geometries": args.batch, "basis": "6-31g*", "atoms": [int(min(len(a) for a in geoms)),
                                                                  int(max(len(a) for a in geoms))],
@@ -252,56 +339,95 @@ def measure_batch(args):
            "jk_ms": tj, "grad_ms": tg, "jk_builds_per_s": args.batch / (tj * 1e-3),
            "grad_evals_per_s": args.batch / (tg * 1e-3),
            "geometry_steps_per_s": args.batch / ((tj + tg) * 1e-3), "setup_s": setup_s,
-           "density": "core-Hamiltonian guess of each geometry (J/K cost depends on the Schwarz lists, not D)"}
+           "mixed": {"cutoff": MIXED_CUTOFF, "jk_ms": tjm, "grad_ms": tgm,
+                     "geometry_steps_per_s": args.batch / ((tjm + tgm) * 1e-3),
+                     "speedup_vs_fp64": (tj + tg) / (tjm + tgm),
+                     "max_energy_error_vs_fp64_ha": dE,
+                     "max_grad_error_vs_fp64_ha_bohr": float((g32 - g64).abs().max().item())},
+           "density": "core-Hamiltonian guess of each geometry"}
     if args.batch_scf:
-        t1 = time.perf_counter()
-        res = scf.run(handoff=0.9, handoff_after=10)
-        torch.cuda.synchronize()
-        t2 = time.perf_counter()
-        scf.gradients()
-        torch.cuda.synchronize()
-        t3 = time.perf_counter()
-        out["scf"] = {"iterations": res.iterations, "converged": int(res.converged.sum()),
-                      "scf_s": t2 - t1, "gradient_s": t3 - t2,
-                      "geometries_per_s": args.batch / (t3 - t1),
-                      "note": "RHF to dE 1e-9, rms dD 1e-7, DIIS error 1e-5; one CUDA graph per iteration "
-                              "(Fock build, DIIS, purification); once 90 % have converged the rest continue "
-                              "in a batch of their own; energy + gradient per geometry"}
+        for name, prec in (("fp64", FP64), ("mixed", MIXED)):
+            eng.set_precision(prec, MIXED_CUTOFF)
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            res = scf.run()
+            t2 = time.perf_counter()
+            out.setdefault("scf", {})[name] = {
+                "iterations": res.iterations, "converged": int(res.converged.sum()), "seconds": t2 - t1,
+                "geometries_per_s": args.batch / (t2 - t1), "energies_head": [float(e) for e in res.energies[:4]]}
+            if name == "fp64":
+                e64, g64s = res.energies.copy(), scf.gradients()
+            else:
+                out["scf"]["mixed"]["max_energy_error_vs_fp64_ha"] = float(np.abs(res.energies - e64).max())
+                out["scf"]["mixed"]["max_grad_error_vs_fp64_ha_bohr"] = float(
+                    max(np.abs(a - b_).max() for a, b_ in zip(scf.gradients(), g64s)))
+        eng.set_precision(FP64)
+        out["scf"]["note"] = ("iqcp_batch_scf: RHF to dE 1e-9, rms dD 1e-7, DIIS error 1e-5 from the core guess, one "
+                              "CUDA graph per iteration (Fock build, DIIS, purification), energy + RHF gradient "
+                              "per geometry, wall time")
     scf.eng.close()
     return out
 
 
 def run_reference(args, rank):
-    """Reference arm: the oracle's CPU restatement, bounded samples per step."""
+    """Reference arm: the oracle's CPU restatement of the reference algorithm,
+    without the product library (basis from oracle/basis.py, geometry and
+    density from the committed fixture).  With K timed steps, step k evaluates
+    the bra shell pairs P with P % K == k, so the K steps together are one full
+    J/K build and one full gradient: no extrapolation."""
     if rank != 0:
         return
-    from iqcp_b200 import BasisSet
-    from iqcp_b200.molecules import workload
     import oracle
-    atoms, basis = workload(WORKLOAD, args.seed)
-    b = BasisSet.build(atoms, basis)
-    rng = np.random.default_rng(args.seed)
-    A = rng.normal(size=(b.n_basis, b.n_basis)) * 0.05
-    D = A + A.T
-    stride = max(args.cpu_sample_stride * 4, 1)
+    from oracle.basis import build_basis
+    fx = load_fixture()
+    b = build_basis(fx["atoms"], fx["basis"])
+    D = fx["D"]
+    stride = max(1, args.steps)
+    wstride = 4 * stride
     for w in range(args.warmup):
-        cpu_baseline(b, D, stride, w % stride)
-    times = []
+        oracle_sample(b, D, wstride, w % wstride)
+    tj = tg = 0.0
     for k in range(args.steps):
-        r = cpu_baseline(b, D, stride, (args.warmup + k) % stride)
-        times.append(1.0 / r["value"])
-    t = float(np.mean(times))
+        a, c = oracle_sample(b, D, stride, k)
+        tj += a
+        tg += c
+    t = tj + tg            # one full step
+    threads = oracle.max_threads()
     line = {"impl": "reference", "metric": METRIC, "value": 1.0 / t, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded molecule)",
             "config": workload_config(b, args.seed),
-            "cpu_baseline": {"value": 1.0 / t, "unit": UNIT, "cores": oracle.max_threads(), "kind": "port",
-                             "sample": "per step: every %d-th bra shell pair (rotating phase), scaled by %d"
-                                       % (stride, stride)},
+            "cpu_baseline": {"value": 1.0 / t, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": "the %d timed steps evaluate the bra shell pairs P with P %% %d == k "
+                                       "(k = 0..%d): together one full J/K build and one full gradient, "
+                                       "extrapolation factor 1" % (args.steps, stride, stride - 1),
+                             "jk_s": tj, "grad_s": tg},
             "e2e": {"value": 1.0 / t, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "note": "the reference's Rust path cannot be built here (no cargo); its algorithm restated in "
-                    "C++ (oracle/) is timed on all host threads"}
+                    "C++ (oracle/) is timed on all host threads; no product library is loaded"}
     print(json.dumps(line), flush=True)
+
+
+def class_table(per_kernel, fl_jk, fl_gr, peak64, modes, executed):
+    """Per (kind, class): live ms per launch, model TFLOP/s and its fraction of
+    the FP64 peak; executed FP64 TFLOP/s where an ncu count of the same kernel
+    variant is on record."""
+    rows = []
+    for (kind, X, Y), (tot, cnt, cls, _) in sorted(per_kernel.items(), key=lambda kv: -kv[1][0]):
+        if kind not in ("jk", "grad"):
+            continue
+        ms = tot / cnt
+        fl = (fl_jk if kind == "jk" else fl_gr)[X, Y]
+        mode = int(modes[0 if kind == "jk" else 1][X][Y])
+        row = {"kernel": "%s %s" % (kind, cls), "mode": mode, "ms": round(ms, 4),
+               "model_tflops": fl / (ms * 1e-3) * 1e-12, "model_frac": fl / (ms * 1e-3) * 1e-12 / peak64}
+        ex = executed.get("%s %s mode %d" % (kind, cls, mode)) if executed else None
+        if ex:
+            row["executed_tflops"] = ex["fp64_flops"] / (ms * 1e-3) * 1e-12
+            row["executed_frac"] = row["executed_tflops"] / peak64
+            row["fp64_pipe_pct_ncu"] = ex.get("fp64_pipe_pct")
+        rows.append(row)
+    return rows
 
 
 def main():
@@ -317,23 +443,20 @@ def main():
     from datetime import timedelta
 
     from iqcp_b200 import BasisSet, FockEngine, measure_peak
-    from iqcp_b200.molecules import workload
     from iqcp_b200.scf import rhf_scf
 
     torch.cuda.set_device(local)
     if world > 1:
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
-    atoms, basis = workload(WORKLOAD, args.seed)
-    b = BasisSet.build(atoms, basis)
+    fx = load_fixture()
+    b = BasisSet.build(fx["atoms"], fx["basis"])
     n = b.n_basis
     stream = torch.cuda.current_stream()
     eng = FockEngine(b, device=local)
     eng.set_stream(stream.cuda_stream)
-    # converged RHF density (set-up, not timed)
     S, T, V = eng.one_electron()
     H = T + V
-    scf = rhf_scf(S, H, b.nuclear_repulsion(), b.n_electrons // 2, eng.build_fock, e_tol=1e-8, d_tol=1e-6)
-    D = scf.density
+    D = fx["D"]
     dD = torch.from_numpy(D).to("cuda")
     dJ = torch.empty_like(dD)
     dK = torch.empty_like(dD)
@@ -343,6 +466,7 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(b, D, args.cpu_sample_stride)
+        cpu["single_thread"] = single_thread_fock(FockEngine, BasisSet)
     peak64 = measure_peak("fp64")
     peak32 = measure_peak("fp32")
 
@@ -397,62 +521,82 @@ def main():
 
     # end to end through the public host-buffer API (pinned host memory)
     hD = torch.from_numpy(D).pin_memory().numpy()
-    hJ = torch.empty((n, n), dtype=torch.float64).pin_memory().numpy()
-    hK = torch.empty((n, n), dtype=torch.float64).pin_memory().numpy()
     e2e_t = 0.0
     for k in range(args.steps):
         flush.zero_()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        J, K = eng.build_jk(hD)
-        g = eng.eri_gradient(hD, 1.0)
+        eng.build_jk(hD)
+        eng.eri_gradient(hD, 1.0)
         e2e_t += time.perf_counter() - t0
     e2e_t = max_over_ranks(e2e_t, world)
     e2e = {"value": job_throughput(world, args.steps, e2e_t), "unit": UNIT,
            "h2d_bytes_per_step": 2 * n * n * 8 + b.n_atoms * 3 * 8,
            "d2h_bytes_per_step": 2 * n * n * 8 + b.n_atoms * 3 * 8}
 
-    mixed = None if args.no_mixed else measure_mixed(args, eng, b, H, D, dD, dJ, dK, dg, flush, stream, world)
+    # FP64 parity at the bench density against the oracle (outside the timed region)
+    F64 = eng.build_fock(H, D)
+    g64 = eng.eri_gradient(D, 1.0)
+    scf = rhf_scf(S, H, b.nuclear_repulsion(), b.n_electrons // 2, eng.build_fock, e_tol=1e-10, d_tol=1e-8, D0=D)
+    fp64 = {"ms_per_step": t_ms / args.steps, "F": F64, "g": g64, "e_at_d": 0.5 * float(np.sum(D * (H + F64)))}
+    mixed = None if args.no_mixed else measure_mixed(args, eng, b, H, S, fx, dD, dJ, dK, dg, flush, stream,
+                                                     world, fp64)
     batch = None
     if world == 1 and args.batch > 0:
         batch = measure_batch(args)
 
-    # roofline of the dominant quartet kernel (FP64 pipe)
-    fl_jk, pq_jk, q_jk = eng.model_flops("jk")
-    fl_gr, pq_gr, q_gr = eng.model_flops("grad")
+    # roofline of the dominant quartet kernel (FP64 pipe) and per class
+    fl_jk, _, _ = eng.model_flops("jk")
+    fl_gr, _, _ = eng.model_flops("grad")
     dom = max(per_kernel.items(), key=lambda kv: kv[1][0])
     (kind, X, Y), (tot_ms, cnt, cls, nq) = dom
     avg_ms = tot_ms / cnt
     flops = (fl_jk if kind == "jk" else fl_gr)[X, Y]
     achieved = flops / (avg_ms * 1e-3) * 1e-12
-    traffic = None
+    traffic = executed = None
     try:
         tr = json.load(open(os.path.join(ROOT, "profiles", "ncu_traffic.json")))
         traffic = tr.get("%s%s" % (kind, cls))
     except (OSError, ValueError):
         pass
+    try:
+        executed = json.load(open(os.path.join(ROOT, "profiles", "ncu_exec_c2.json")))["kernels"]
+    except (OSError, ValueError, KeyError):
+        pass
+    classes = class_table(per_kernel, fl_jk, fl_gr, peak64, modes, executed)
+    dom_row = next((r for r in classes if r["kernel"] == "%s %s" % (kind, cls)), {})
     total_model = float(fl_jk.sum() + fl_gr.sum())
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded 40-atom molecule, converged RHF density)",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded 40-atom molecule, oracle-converged RHF "
+                                                   "density)",
         "config": workload_config(b, args.seed),
         "jk_builds_per_s_fp64": None, "grad_evals_per_s_fp64": None,
         "e2e": e2e,
         "roofline": {"bound": "fp64", "kernel": "%s %s" % (kind, cls), "achieved": achieved, "peak": peak64,
                      "unit": "TFLOP/s", "frac": achieved / peak64, "traffic": traffic,
+                     "executed_tflops": dom_row.get("executed_tflops"), "executed_frac": dom_row.get("executed_frac"),
                      "peak_source": "measured live: DFMA throughput probe (iqcp_measure_peak); "
                                     "MEASURED_PEAKS.json has no FP64 figure",
-                     "flops_model": "closed-form per surviving primitive quartet (host.cu class_cost)",
+                     "flops_model": "closed-form per surviving primitive quartet (host.cu class_cost); executed: "
+                                    "ncu DFMA x2 + DMUL + DADD of the same kernel variant "
+                                    "(profiles/ncu_exec_c2.json) over the live launch time",
                      "avg_launch_ms": avg_ms},
+        "roofline_classes": classes,
         "step_model_tflops": total_model / (t_ms / args.steps * 1e-3) * 1e-12,
         "fp32_peak_tflops": peak32,
         "clocks": clocks, "gpu_launches": launches,
         "kernels": {"%s %s" % (k[0], v[2]): round(v[0] / v[1], 4) for k, v in sorted(per_kernel.items())},
-        "scf": {"energy": scf.energy, "iterations": scf.iterations, "converged": bool(scf.converged)},
+        "scf": {"energy": scf.energy, "iterations": scf.iterations, "converged": bool(scf.converged),
+                "oracle_energy": fx["energy"], "energy_error_vs_oracle_ha": abs(scf.energy - fx["energy"])},
+        "parity_fp64": {"grad_2e_max_error_vs_oracle_ha_bohr": float(np.abs(g64 - fx["grad_2e"]).max()),
+                        "scf_energy_error_vs_oracle_ha": abs(scf.energy - fx["energy"])},
         "kernel_modes": {"jk": modes[0].tolist(), "grad": modes[1].tolist(),
-                         "legend": "rows bra class, cols ket class (ss ps pp ds dp dd); 0 thread/quartet, "
-                                   "1 warp/quartet, 2 8 lanes/quartet, 3 32 lanes/quartet"},
+                         "legend": "rows bra class, cols ket class (ss ps pp ds dp dd); J/K: 0 thread/quartet, "
+                                   "1 warp/quartet, 2 / 3 8 / 32 lanes per quartet; gradient: 0 thread/quartet, "
+                                   "1 warp/quartet, 2 thread/quartet with the D x D weights in shared memory, "
+                                   "3 32 lanes per quartet over (primitive quartet, root) items"},
     }
     jk_ms = sum(v[0] / v[1] for k, v in per_kernel.items() if k[0] == "jk")
     gr_ms = sum(v[0] / v[1] for k, v in per_kernel.items() if k[0] == "grad")

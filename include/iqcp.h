@@ -176,6 +176,28 @@ int iqcp_fock_device(iqcp_ctx* ctx, const double* d_H, const double* d_D, double
 int iqcp_jk_device_noalloc(iqcp_ctx* ctx, const double* d_D, double* d_J, double* d_K);
 
 /*
+ * J and K of nset densities at once, each quartet evaluated once and
+ * digested into every density: J_s, K_s of D_s for s < nset.  The matrices
+ * of density s start at element s * P, P = nbf*nbf (or the packed size of a
+ * batched context, see iqcp_batch_layout); each D_s must be symmetric.  This
+ * is the J/K of the CPHF response densities: gen_vind_rhf / gen_vind_rhf_vo
+ * (scf/cphf.rs:828-990) form dm1 = dm + dm^T per trial vector and build J, K
+ * from it one density at a time.  FP64 quadrature whatever the context's
+ * precision.  K may be NULL.  Host buffers, or device pointers for the
+ * _device form (enqueued on the context stream, like iqcp_jk_device).
+ */
+int iqcp_jk_multi(iqcp_ctx* ctx, int nset, const double* D, double* J, double* K);
+int iqcp_jk_multi_device(iqcp_ctx* ctx, int nset, const double* d_D, double* d_J, double* d_K);
+
+/*
+ * The four matrices of compute_fock_decomposition (scf/fock.rs:104-179), host
+ * buffers: J, K, G = J - 1/2 k_scale K and F = H + G (k_scale = 1 for RHF).
+ * Any output may be NULL; H may be NULL when F is.
+ */
+int iqcp_fock_decomposition(iqcp_ctx* ctx, const double* H, const double* D, double k_scale, double* J, double* K,
+                            double* G, double* F);
+
+/*
  * Two-electron part of the nuclear gradient, host buffers:
  * grad[3*atom + dir] += sum over unique quartets of w * d(ij|kl)/dR with
  * w = sum_perm [1/2 D_ij D_kl - 1/4 hf_frac D_ik D_jl].
@@ -185,6 +207,33 @@ int iqcp_jk_device_noalloc(iqcp_ctx* ctx, const double* d_D, double* d_J, double
  */
 int iqcp_eri_grad(iqcp_ctx* ctx, const double* D, double hf_frac, double* grad);
 int iqcp_eri_grad_device(iqcp_ctx* ctx, const double* d_D, double hf_frac, double* d_grad);
+
+/*
+ * Batched RHF to self-consistency on the device: every geometry of the
+ * context (batched or single) iterates together, one CUDA graph replay per
+ * iteration (Fock build, energy, DIIS on X^T (FDS - SDF) X, density by
+ * canonical purification of X^T F X), with X = S^-1/2 from a Newton-Schulz
+ * iteration and the core-Hamiltonian guess unless D0 is given.  Replaces the
+ * per-geometry rhf_scf loop (scf/mod.rs:1363-1586) of the optimiser and scan
+ * callers (optimizer/mod.rs:274-320).  Converged when |dE| < e_tol, rms dD <
+ * d_tol and max |DIIS error| < err_tol (scf/mod.rs:1508-1520).  Host buffers,
+ * packed per geometry as in iqcp_create_batch: D0 (NULL: core guess),
+ * energies[n_mol], converged[n_mol] (0/1), iterations, D_out (packed, may be
+ * NULL) and grad (n_atoms x 3, overwritten with the RHF gradient at the final
+ * density; may be NULL).  max_iter = 0 returns the starting density only.
+ * Closed shells only.  Device scratch is allocated for the call and freed.
+ */
+typedef struct iqcp_scf_options {
+  double e_tol;       /* 1e-9 Ha */
+  double d_tol;       /* 1e-7, rms density change */
+  double err_tol;     /* 1e-5, largest DIIS error element */
+  int max_iter;       /* 80 */
+  int diis_size;      /* 8 (1..16) */
+  int purify_iters;   /* 64 canonical-purification steps per iteration */
+} iqcp_scf_options;
+void iqcp_scf_default_options(iqcp_scf_options* opts);
+int iqcp_batch_scf(iqcp_ctx* ctx, const iqcp_scf_options* opts, const double* D0, double* energies,
+                   int* converged, int* iterations, double* D_out, double* grad);
 
 /*
  * All unique ERIs in the reference's 8-fold compressed layout,

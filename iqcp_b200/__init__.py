@@ -24,8 +24,8 @@ import os
 
 import numpy as np
 
-__all__ = ["BasisSet", "FockEngine", "IqcpError", "boys_eval_all", "rys_roots", "lib_path",
-           "load_library", "ANGSTROM_TO_BOHR", "FP64", "MIXED"]
+__all__ = ["BasisSet", "FockEngine", "BatchFockEngine", "IqcpError", "ScfOptions", "boys_eval_all", "rys_roots",
+           "lib_path", "load_library", "ANGSTROM_TO_BOHR", "FP64", "MIXED"]
 
 ANGSTROM_TO_BOHR = 1.8897261245650618  # constants.rs:63
 FP64, MIXED = 0, 1
@@ -59,6 +59,12 @@ class _BasisDesc(ctypes.Structure):
 class _Options(ctypes.Structure):
     _fields_ = [("schwarz_threshold", ctypes.c_double), ("prim_threshold", ctypes.c_double),
                 ("precision", ctypes.c_int), ("mixed_cutoff", ctypes.c_double), ("device", ctypes.c_int)]
+
+
+class ScfOptions(ctypes.Structure):
+    """iqcp_scf_options of include/iqcp.h."""
+    _fields_ = [("e_tol", ctypes.c_double), ("d_tol", ctypes.c_double), ("err_tol", ctypes.c_double),
+                ("max_iter", ctypes.c_int), ("diis_size", ctypes.c_int), ("purify_iters", ctypes.c_int)]
 
 
 def lib_path():
@@ -107,6 +113,14 @@ EXPORTS = {
     "iqcp_create_batch": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_BasisDesc), ctypes.POINTER(_Options),
                                          ctypes.POINTER(ctypes.c_void_p)]),
     "iqcp_batch_layout": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong), _c_int_p, _c_int_p]),
+    "iqcp_jk_multi": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _c_dbl_p, _c_dbl_p, _c_dbl_p]),
+    "iqcp_jk_multi_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                            ctypes.c_void_p]),
+    "iqcp_fock_decomposition": (ctypes.c_int, [ctypes.c_void_p, _c_dbl_p, _c_dbl_p, ctypes.c_double, _c_dbl_p,
+                                               _c_dbl_p, _c_dbl_p, _c_dbl_p]),
+    "iqcp_scf_default_options": (None, [ctypes.POINTER(ScfOptions)]),
+    "iqcp_batch_scf": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ScfOptions), _c_dbl_p, _c_dbl_p, _c_int_p,
+                                      _c_int_p, _c_dbl_p, _c_dbl_p]),
 }
 
 PAIR_CLASSES = ["ss", "ps", "pp", "ds", "dp", "dd"]
@@ -272,6 +286,28 @@ class FockEngine:
         F = np.empty_like(D)
         self._check(self._lib.iqcp_fock(self._h, _dp(H), _dp(D), float(k_scale), _dp(F)))
         return F
+
+    def build_jk_multi(self, Ds, with_k=True):
+        """J and K of several symmetric densities with one pass over the quartets
+        (iqcp_jk_multi): the response-density J/K of gen_vind_rhf (scf/cphf.rs:828)."""
+        D = np.ascontiguousarray(np.stack([self._mat(d) for d in Ds]))
+        J = np.empty_like(D)
+        K = np.empty_like(D) if with_k else None
+        self._check(self._lib.iqcp_jk_multi(self._h, len(D), _dp(D), _dp(J), _dp(K) if with_k else None))
+        return (list(J), list(K)) if with_k else list(J)
+
+    def jk_multi_device(self, nset, d_D, d_J, d_K=None):
+        self._check(self._lib.iqcp_jk_multi_device(self._h, int(nset), ctypes.c_void_p(d_D), ctypes.c_void_p(d_J),
+                                                   ctypes.c_void_p(d_K) if d_K else None))
+
+    def fock_decomposition(self, H, D, k_scale=1.0):
+        """(J, K, G, F) with G = J - k_scale/2 K, F = H + G: compute_fock_decomposition
+        (scf/fock.rs:104-179)."""
+        H, D = self._mat(H), self._mat(D)
+        J, K, G, F = (np.empty_like(D) for _ in range(4))
+        self._check(self._lib.iqcp_fock_decomposition(self._h, _dp(H), _dp(D), float(k_scale), _dp(J), _dp(K),
+                                                      _dp(G), _dp(F)))
+        return J, K, G, F
 
     def eri_gradient(self, D, hf_frac=1.0):
         D = self._mat(D)
@@ -458,6 +494,18 @@ class BatchFockEngine(FockEngine):
         K = np.empty_like(D) if with_k else None
         self._check(self._lib.iqcp_jk(self._h, _dp(D), _dp(J), _dp(K) if with_k else None))
         return (self.unpack(J), self.unpack(K)) if with_k else self.unpack(J)
+
+    def build_jk_multi(self, sets, with_k=True):
+        """sets[s] = per-molecule densities of response set s -> (J sets, K sets)."""
+        D = np.ascontiguousarray(np.stack([self.pack(Ds) for Ds in sets]))
+        J = np.empty_like(D)
+        K = np.empty_like(D) if with_k else None
+        self._check(self._lib.iqcp_jk_multi(self._h, len(D), _dp(D), _dp(J), _dp(K) if with_k else None))
+        Js = [self.unpack(x) for x in J]
+        return (Js, [self.unpack(x) for x in K]) if with_k else Js
+
+    def fock_decomposition(self, H, D, k_scale=1.0):
+        raise IqcpError(-1, "use build_jk on a batched context")
 
     def build_fock(self, Hs, Ds, k_scale=1.0):
         H, D = self.pack(Hs), self.pack(Ds)

@@ -137,6 +137,8 @@ struct JKArgs {
   int* next_task;             // work counter (zeroed before the launch)
   const long long* mol_base;  // per molecule: offset of its nbf x nbf block in D, J, K
   const int* mol_n;           // per molecule: nbf (row stride of its block)
+  int nset;                   // densities digested per quartet (1, or several response densities)
+  long long set_stride;       // elements between consecutive densities in D, J and K
 };
 
 struct StoreArgs {

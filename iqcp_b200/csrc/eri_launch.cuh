@@ -2,7 +2,7 @@
 // Classes with many components use the warp-cooperative kernels
 // (eri_team.cuh); the small ones keep one quartet per thread.
 #pragma once
-#include "eri_team.cuh"
+#include "eri_group.cuh"
 
 namespace iqcp {
 
@@ -38,7 +38,8 @@ inline int persistent_blocks(K kernel, size_t smem, int ntasks, int threads = 12
 
 // mode: 0 one quartet per thread, 1 warp-cooperative (eri_team.cuh),
 // 2 / 3 eight / thirty-two lanes share one quartet's primitive quartets
-// (small classes only; larger classes fall back to mode 0).  The FP32 share
+// (J/K: small classes only; gradient: see launch_grad_variant; requests a
+// class has no kernel for fall back to mode 0).  The FP32 share
 // of a mixed call (pass 2) has modes 0 (up to 324 components), 1, and 2 for
 // the small classes; other requests map onto those.
 template <typename R, int LA, int LB, int LC, int LD>
@@ -81,30 +82,45 @@ inline size_t max_smem_optin() {
   return (size_t)v;
 }
 
+// Gradient variants: mode 2 is one quartet per thread with the D x D weights
+// in shared memory (classes of kWshMinComp..kWshMaxComp components; others map
+// to mode 0), mode 3 the grouped kernel of eri_group.cuh (up to
+// kGroupGradMaxComp components, 32 lanes per quartet; the FP32 share uses 8).
+constexpr int kWshMinComp = 18, kWshMaxComp = 108;
+constexpr int kGroupGradMaxComp = 108;
+
 template <typename R, int LA, int LB, int LC, int LD>
 cudaError_t launch_grad_variant(const GradArgs& args, cudaStream_t st) {
   using C = Cls<LA, LB, LC, LD>;
   constexpr bool F32 = sizeof(R) == 4;
   constexpr int NRG = (LA + LB + LC + LD + 2) / 2 + 1;
+  constexpr bool WSH_OK = !F32 && C::NCOMP >= kWshMinComp && C::NCOMP <= kWshMaxComp;
   using TG = TeamGrad2<LA, LB, LC, LD>;
   const bool team = args.mode == 1 || (F32 && C::NCOMP > 324);
+  const bool wsh = !team && args.mode == 2 && WSH_OK;
+  const bool group = !team && !wsh && (args.mode == 3 || (F32 && args.mode == 2)) && C::NCOMP <= kGroupGradMaxComp;
   // the team variant reads the Rys coefficients through L1 (no staged table)
-  const size_t fixed = team ? sizeof(double) * TG::WPB * TG::PER_WARP : sizeof(double) * rys_tab_doubles<NRG>();
+  size_t fixed = sizeof(double) * rys_tab_doubles<NRG>();
+  if (team) fixed = sizeof(double) * TG::WPB * TG::PER_WARP;
+  else if (wsh) fixed += sizeof(R) * grad_wsh_doubles<LA, LB, LC, LD>();
+  else if (group)
+    fixed += sizeof(double) * (F32 ? GroupGrad<R, LA, LB, LC, LD, 8>::WDOUBLES : GroupGrad<R, LA, LB, LC, LD, 32>::WDOUBLES);
   // the per-block gradient accumulator only when it fits beside the tables
   GradArgs a = args;
   if (a.gsmem && fixed + sizeof(double) * 3 * a.natoms > max_smem_optin()) a.gsmem = 0;
   const size_t gacc = a.gsmem ? sizeof(double) * 3 * a.natoms : 0;
-  const size_t tb = sizeof(double) * rys_tab_doubles<NRG>() + gacc;
+  const size_t bytes = fixed + gacc;
   if (team) {
-    const size_t bytes = sizeof(double) * TG::WPB * TG::PER_WARP + gacc;
     IQCP_LAUNCH_T((grad_team2_kernel<R, LA, LB, LC, LD>), 32 * TG::WPB, bytes, a, st);
-  } else if (C::NCOMP <= 36 && (a.mode == 2 || a.mode == 3)) {
-    if constexpr (C::NCOMP <= 36) {
-      if (a.mode == 2 || F32) IQCP_LAUNCH((grad_kernel<R, LA, LB, LC, LD, 8>), tb, a, st);
-      else IQCP_LAUNCH((grad_kernel<R, LA, LB, LC, LD, 32>), tb, a, st);
+  } else if (wsh) {
+    if constexpr (WSH_OK) IQCP_LAUNCH((grad_kernel<R, LA, LB, LC, LD, 1, true>), bytes, a, st);
+  } else if (group) {
+    if constexpr (C::NCOMP <= kGroupGradMaxComp) {
+      if (F32) IQCP_LAUNCH((grad_group_kernel<R, LA, LB, LC, LD, 8>), bytes, a, st);
+      else IQCP_LAUNCH((grad_group_kernel<R, LA, LB, LC, LD, 32>), bytes, a, st);
     }
   } else if constexpr (!F32 || C::NCOMP <= 324) {
-    IQCP_LAUNCH((grad_kernel<R, LA, LB, LC, LD, 1>), tb, a, st);
+    IQCP_LAUNCH((grad_kernel<R, LA, LB, LC, LD, 1>), bytes, a, st);
   }
   return cudaGetLastError();
 }

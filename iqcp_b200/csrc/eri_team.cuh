@@ -18,6 +18,13 @@
 
 namespace iqcp {
 
+// Component ax (runtime) of a 3-vector without indexing it: an indexed
+// access would place the vector -- and the ShellPair / PrimPair it belongs to --
+// in local memory.
+__device__ __forceinline__ double pick3(int ax, double x, double y, double z) {
+  return ax == 0 ? x : (ax == 1 ? y : z);
+}
+
 // Rule for one root r of an N-point rule (phase A lanes each need one root).
 // (table staged in shared memory at s)
 template <int N>
@@ -75,11 +82,13 @@ __device__ __forceinline__ void team_prim_loop(const JKArgs& args, const ShellPa
         rys_rule_one<NR>(T, r, rtab, &t2, &wr);
         const double b00 = 0.5 * t2 * inv_s, h = 0.5 - 0.5 * t2;
         const double b10 = fma(h, pb.inv_p, b00), b01 = fma(h, pk.inv_p, b00);
-        const double pa = pb.P[ax] - bp.A[ax], qc = pk.P[ax] - kp.A[ax];
+        const double pa = pick3(ax, pb.P[0] - bp.A[0], pb.P[1] - bp.A[1], pb.P[2] - bp.A[2]);
+        const double qc = pick3(ax, pk.P[0] - kp.A[0], pk.P[1] - kp.A[1], pk.P[2] - kp.A[2]);
+        const double pq = pick3(ax, PQ[0], PQ[1], PQ[2]);
         const double g00 = ax == 2 ? wr * kTwoPi52 * pb.cK * pk.cK * pb.inv_p * pk.inv_p * rs : 1.0;
         axis_table<R, C::NBRA, C::NKET, LA, LB, LC, LD>(
-            R(pa - t2 * q * inv_s * PQ[ax]), R(qc + t2 * p * inv_s * PQ[ax]), R(b00), R(b10), R(b01), R(AB[ax]),
-            R(CD[ax]), R(g00), tab + (r * 3 + ax) * TSZ);
+            R(pa - t2 * q * inv_s * pq), R(qc + t2 * p * inv_s * pq), R(b00), R(b10), R(b01),
+            R(pick3(ax, AB[0], AB[1], AB[2])), R(pick3(ax, CD[0], CD[1], CD[2])), R(g00), tab + (r * 3 + ax) * TSZ);
       }
       __syncwarp();
 #pragma unroll
@@ -168,73 +177,90 @@ __global__ void __launch_bounds__(128) jk_team_kernel(JKArgs args) {
       const int comp = lane + 32 * m;
       if (comp < C::NCOMP) work[comp] = f * acc[m];
     }
-    for (int i = lane; i < C::NC * C::ND; i += 32) Dcd[i] = __ldg(D + (kp.oa + i / C::ND) * n + kp.ob + i % C::ND);
-    if (DO_K) {
-      for (int i = lane; i < C::NB * C::ND; i += 32) Dbd[i] = __ldg(D + (bp.ob + i / C::ND) * n + kp.ob + i % C::ND);
-      for (int i = lane; i < C::NA * C::ND; i += 32) Dad[i] = __ldg(D + (bp.oa + i / C::ND) * n + kp.ob + i % C::ND);
-      for (int i = lane; i < C::NB * C::NC; i += 32) Dbc[i] = __ldg(D + (bp.ob + i / C::NC) * n + kp.oa + i % C::NC);
-      for (int i = lane; i < C::NA * C::NC; i += 32) Dac[i] = __ldg(D + (bp.oa + i / C::NC) * n + kp.oa + i % C::NC);
+    // every density of the call (nset > 1: response densities) is digested
+    // with the same integrals
+    for (int s = 0; s < args.nset; ++s) {
+      const double* __restrict__ Dm = D + s * args.set_stride;
+      double* Jm = args.J + mb + s * args.set_stride;
+      double* Km = DO_K ? args.K + mb + s * args.set_stride : nullptr;
+      if (s > 0) {  // the bra block of this density (set 0's was staged per task)
+        __syncwarp();
+        for (int i = lane; i < C::NA * C::NB; i += 32)
+          Dab[i] = __ldg(Dm + (bp.oa + i / C::NB) * n + bp.ob + i % C::NB);
+      }
+      for (int i = lane; i < C::NC * C::ND; i += 32) Dcd[i] = __ldg(Dm + (kp.oa + i / C::ND) * n + kp.ob + i % C::ND);
+      if (DO_K) {
+        for (int i = lane; i < C::NB * C::ND; i += 32) Dbd[i] = __ldg(Dm + (bp.ob + i / C::ND) * n + kp.ob + i % C::ND);
+        for (int i = lane; i < C::NA * C::ND; i += 32) Dad[i] = __ldg(Dm + (bp.oa + i / C::ND) * n + kp.ob + i % C::ND);
+        for (int i = lane; i < C::NB * C::NC; i += 32) Dbc[i] = __ldg(Dm + (bp.ob + i / C::NC) * n + kp.oa + i % C::NC);
+        for (int i = lane; i < C::NA * C::NC; i += 32) Dac[i] = __ldg(Dm + (bp.oa + i / C::NC) * n + kp.oa + i % C::NC);
+      }
+      __syncwarp();
+      // J~_ab += 2 sum_cd I D_cd
+      for (int ab = lane; ab < C::NA * C::NB; ab += 32) {
+        double v = 0.0;
+#pragma unroll
+        for (int cd = 0; cd < C::NC * C::ND; ++cd) v = fma(work[ab * C::NC * C::ND + cd], Dcd[cd], v);
+        atomicAdd(Jm + (bp.oa + ab / C::NB) * n + bp.ob + ab % C::NB, 2.0 * v);
+      }
+      // J~_cd += 2 sum_ab I D_ab
+      for (int cd = lane; cd < C::NC * C::ND; cd += 32) {
+        double v = 0.0;
+#pragma unroll
+        for (int ab = 0; ab < C::NA * C::NB; ++ab) v = fma(work[ab * C::NC * C::ND + cd], Dab[ab], v);
+        atomicAdd(Jm + (kp.oa + cd / C::ND) * n + kp.ob + cd % C::ND, 2.0 * v);
+      }
+      if (DO_K) {
+        // K~_ac += sum_bd I D_bd
+        for (int x = lane; x < C::NA * C::NC; x += 32) {
+          const int a = x / C::NC, c = x % C::NC;
+          double v = 0.0;
+#pragma unroll
+          for (int b = 0; b < C::NB; ++b)
+#pragma unroll
+            for (int d = 0; d < C::ND; ++d)
+              v = fma(work[((a * C::NB + b) * C::NC + c) * C::ND + d], Dbd[b * C::ND + d], v);
+          atomicAdd(Km + (bp.oa + a) * n + kp.oa + c, v);
+        }
+        // K~_bc += sum_ad I D_ad
+        for (int x = lane; x < C::NB * C::NC; x += 32) {
+          const int b = x / C::NC, c = x % C::NC;
+          double v = 0.0;
+#pragma unroll
+          for (int a = 0; a < C::NA; ++a)
+#pragma unroll
+            for (int d = 0; d < C::ND; ++d)
+              v = fma(work[((a * C::NB + b) * C::NC + c) * C::ND + d], Dad[a * C::ND + d], v);
+          atomicAdd(Km + (bp.ob + b) * n + kp.oa + c, v);
+        }
+        // K~_ad += sum_bc I D_bc
+        for (int x = lane; x < C::NA * C::ND; x += 32) {
+          const int a = x / C::ND, d = x % C::ND;
+          double v = 0.0;
+#pragma unroll
+          for (int b = 0; b < C::NB; ++b)
+#pragma unroll
+            for (int c = 0; c < C::NC; ++c)
+              v = fma(work[((a * C::NB + b) * C::NC + c) * C::ND + d], Dbc[b * C::NC + c], v);
+          atomicAdd(Km + (bp.oa + a) * n + kp.ob + d, v);
+        }
+        // K~_bd += sum_ac I D_ac
+        for (int x = lane; x < C::NB * C::ND; x += 32) {
+          const int b = x / C::ND, d = x % C::ND;
+          double v = 0.0;
+#pragma unroll
+          for (int a = 0; a < C::NA; ++a)
+#pragma unroll
+            for (int c = 0; c < C::NC; ++c)
+              v = fma(work[((a * C::NB + b) * C::NC + c) * C::ND + d], Dac[a * C::NC + c], v);
+          atomicAdd(Km + (bp.ob + b) * n + kp.ob + d, v);
+        }
+      }
+      __syncwarp();
     }
-    __syncwarp();
-    // J~_ab += 2 sum_cd I D_cd
-    for (int ab = lane; ab < C::NA * C::NB; ab += 32) {
-      double v = 0.0;
-#pragma unroll
-      for (int cd = 0; cd < C::NC * C::ND; ++cd) v = fma(work[ab * C::NC * C::ND + cd], Dcd[cd], v);
-      atomicAdd((args.J + mb) + (bp.oa + ab / C::NB) * n + bp.ob + ab % C::NB, 2.0 * v);
-    }
-    // J~_cd += 2 sum_ab I D_ab
-    for (int cd = lane; cd < C::NC * C::ND; cd += 32) {
-      double v = 0.0;
-#pragma unroll
-      for (int ab = 0; ab < C::NA * C::NB; ++ab) v = fma(work[ab * C::NC * C::ND + cd], Dab[ab], v);
-      atomicAdd((args.J + mb) + (kp.oa + cd / C::ND) * n + kp.ob + cd % C::ND, 2.0 * v);
-    }
-    if (DO_K) {
-      // K~_ac += sum_bd I D_bd
-      for (int x = lane; x < C::NA * C::NC; x += 32) {
-        const int a = x / C::NC, c = x % C::NC;
-        double v = 0.0;
-#pragma unroll
-        for (int b = 0; b < C::NB; ++b)
-#pragma unroll
-          for (int d = 0; d < C::ND; ++d)
-            v = fma(work[((a * C::NB + b) * C::NC + c) * C::ND + d], Dbd[b * C::ND + d], v);
-        atomicAdd((args.K + mb) + (bp.oa + a) * n + kp.oa + c, v);
-      }
-      // K~_bc += sum_ad I D_ad
-      for (int x = lane; x < C::NB * C::NC; x += 32) {
-        const int b = x / C::NC, c = x % C::NC;
-        double v = 0.0;
-#pragma unroll
-        for (int a = 0; a < C::NA; ++a)
-#pragma unroll
-          for (int d = 0; d < C::ND; ++d)
-            v = fma(work[((a * C::NB + b) * C::NC + c) * C::ND + d], Dad[a * C::ND + d], v);
-        atomicAdd((args.K + mb) + (bp.ob + b) * n + kp.oa + c, v);
-      }
-      // K~_ad += sum_bc I D_bc
-      for (int x = lane; x < C::NA * C::ND; x += 32) {
-        const int a = x / C::ND, d = x % C::ND;
-        double v = 0.0;
-#pragma unroll
-        for (int b = 0; b < C::NB; ++b)
-#pragma unroll
-          for (int c = 0; c < C::NC; ++c)
-            v = fma(work[((a * C::NB + b) * C::NC + c) * C::ND + d], Dbc[b * C::NC + c], v);
-        atomicAdd((args.K + mb) + (bp.oa + a) * n + kp.ob + d, v);
-      }
-      // K~_bd += sum_ac I D_ac
-      for (int x = lane; x < C::NB * C::ND; x += 32) {
-        const int b = x / C::ND, d = x % C::ND;
-        double v = 0.0;
-#pragma unroll
-        for (int a = 0; a < C::NA; ++a)
-#pragma unroll
-          for (int c = 0; c < C::NC; ++c)
-            v = fma(work[((a * C::NB + b) * C::NC + c) * C::ND + d], Dac[a * C::NC + c], v);
-        atomicAdd((args.K + mb) + (bp.ob + b) * n + kp.ob + d, v);
-      }
+    if (args.nset > 1) {  // restore set 0's bra block for the next ket
+      for (int i = lane; i < C::NA * C::NB; i += 32)
+        Dab[i] = __ldg(D + (bp.oa + i / C::NB) * n + bp.ob + i % C::NB);
     }
     __syncwarp();
   }
@@ -248,8 +274,8 @@ __global__ void __launch_bounds__(128) jk_team_kernel(JKArgs args) {
 // Tables are extended by one on A, B and C (the D derivative follows from
 // translational invariance, dD = -(dA + dB + dC)), with one more root than the
 // energy (eri/mod.rs:2146-2149).  Per surviving primitive quartet:
-//   phase A   lanes 0 .. 3*NR-1 build the extended 1D tables E of their
-//             (root, axis) in shared memory;
+//   phase A   the lanes build the extended 1D tables E of every (root, axis)
+//             in shared memory, one row a of a table per lane (axis_slice);
 //   phase A2  all 32 lanes turn them into, for every unextended index
 //             (ia, ib, ic, id), the four values I, dI/dA, dI/dB, dI/dC
 //             (d/dA: 2a E(ia+1) - ia E(ia-1), likewise B, C), stored as two
@@ -307,6 +333,11 @@ struct TeamGrad2 {
   static constexpr int PER_WARP = TAB + QT + ((DBLK + 3) / 4) * 4;
   static constexpr int CPL = (C::NCOMP + 31) / 32;
   static constexpr int WPB = team_warps_per_block(PER_WARP);
+  // resident blocks per SM asked of the compiler: what shared memory allows,
+  // but no more than leaves 168 registers per thread (65536 / (MINB * 32 * WPB))
+  static constexpr int SMB = team_resident(WPB, PER_WARP) / WPB;
+  static constexpr int RGB = 65536 / (168 * 32 * WPB);
+  static constexpr int MINB = (SMB < RGB ? SMB : RGB) > 0 ? (SMB < RGB ? SMB : RGB) : 1;
   __host__ __device__ static constexpr int eidx(int a, int b, int c, int d) {
     return ((a * (EB + 1) + b) * (EC + 1) + c) * (ED + 1) + d;
   }
@@ -320,7 +351,8 @@ template <> struct Vec2<double> { using type = double2; };
 template <> struct Vec2<float> { using type = float2; };
 
 template <typename R, int LA, int LB, int LC, int LD>
-__global__ void __launch_bounds__(32 * TeamGrad2<LA, LB, LC, LD>::WPB) grad_team2_kernel(GradArgs args) {
+__global__ void __launch_bounds__(32 * TeamGrad2<LA, LB, LC, LD>::WPB, TeamGrad2<LA, LB, LC, LD>::MINB)
+grad_team2_kernel(GradArgs args) {
   using C = Cls<LA, LB, LC, LD>;
   using TG = TeamGrad2<LA, LB, LC, LD>;
   using V2 = typename Vec2<R>::type;
@@ -429,8 +461,10 @@ __global__ void __launch_bounds__(32 * TeamGrad2<LA, LB, LC, LD>::WPB) grad_team
         const PrimPair pk = load_pp(args.pp + kp.pstart + j);
         if (pb.K * pk.K < args.prim_thr) continue;
         __syncwarp();
-        if (lane < 3 * NR) {
-          const int r = lane / 3, ax = lane - 3 * r;
+        // phase A: (root, axis, row a) slices of the extended tables, one per lane
+        for (int task = lane; task < 3 * NR * (TG::EA + 1); task += 32) {
+          const int a = task / (3 * NR), t = task - a * (3 * NR);
+          const int r = t / 3, ax = t - 3 * r;
           const double p = pb.p, q = pk.p, s = p + q;
           const double PQ[3] = {pb.P[0] - pk.P[0], pb.P[1] - pk.P[1], pb.P[2] - pk.P[2]};
           const double rs = rsqrt(s), inv_s = rs * rs;  // 1/(p+q), 1/sqrt(p+q): one rsqrt
@@ -440,11 +474,23 @@ __global__ void __launch_bounds__(32 * TeamGrad2<LA, LB, LC, LD>::WPB) grad_team
           rys_rule_one_g<NR>(T, r, &t2, &wr);
           const double b00 = 0.5 * t2 * inv_s, h = 0.5 - 0.5 * t2;
           const double b10 = fma(h, pb.inv_p, b00), b01 = fma(h, pk.inv_p, b00);
-          const double pa = pb.P[ax] - bp.A[ax], qc = pk.P[ax] - kp.A[ax];
+          const double pa = pick3(ax, pb.P[0] - bp.A[0], pb.P[1] - bp.A[1], pb.P[2] - bp.A[2]);
+          const double qc = pick3(ax, pk.P[0] - kp.A[0], pk.P[1] - kp.A[1], pk.P[2] - kp.A[2]);
+          const double pq = pick3(ax, PQ[0], PQ[1], PQ[2]);
           const double g00 = ax == 2 ? wr * kTwoPi52 * pb.cK * pk.cK * pb.inv_p * pk.inv_p * rs : 1.0;
-          axis_table<R, LA + LB + 1, LC + LD + 1, TG::EA, TG::EB, TG::EC, TG::ED>(
-              R(pa - t2 * q * inv_s * PQ[ax]), R(qc + t2 * p * inv_s * PQ[ax]), R(b00), R(b10), R(b01), R(AB[ax]),
-              R(CD[ax]), R(g00), tab + (r * 3 + ax) * TSZ);
+          const R c00 = R(pa - t2 * q * inv_s * pq), c0p = R(qc + t2 * p * inv_s * pq);
+          const R abx = R(pick3(ax, AB[0], AB[1], AB[2])), cdx = R(pick3(ax, CD[0], CD[1], CD[2]));
+          R* dst = tab + t * TSZ;
+#define IQCP_SLICE(AV)                                                                                  \
+  axis_slice<R, LA + LB + 1, LC + LD + 1, TG::EA, TG::EB, TG::EC, TG::ED, AV>(                          \
+      c00, c0p, R(b00), R(b10), R(b01), abx, cdx, R(g00), dst)
+          if (a == 0) IQCP_SLICE(0);
+          else if (a == 1) IQCP_SLICE(1);
+          else if constexpr (TG::EA >= 2) {
+            if (a == 2) IQCP_SLICE((TG::EA >= 2 ? 2 : 0));
+            else if constexpr (TG::EA >= 3) IQCP_SLICE((TG::EA >= 3 ? 3 : 0));
+          }
+#undef IQCP_SLICE
         }
         __syncwarp();
         // phase A2: I, dI/dA, dI/dB, dI/dC on the unextended indices

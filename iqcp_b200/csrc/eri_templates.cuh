@@ -90,6 +90,61 @@ __device__ __forceinline__ void axis_table(R c00, R c0p, R b00, R b10, R b01, R 
     }
 }
 
+// Row a = A of axis_table's output, I[A][b][c][d] for every b, c, d, with the
+// same recurrences in the same order (so the entries are bitwise those of
+// axis_table): the VRR up to row min(A + IB, NB), the bra transfer only for
+// the rows A..A+IB it feeds, the ket transfer for row A.  Lets several lanes
+// share one table with a fraction of the registers.
+template <typename R, int NB, int NK, int IA, int IB, int IC, int ID, int A>
+__device__ __forceinline__ void axis_slice(R c00, R c0p, R b00, R b10, R b01, R ab, R cd, R g00,
+                                           R* __restrict__ I) {
+  constexpr int NT = (A + IB < NB) ? A + IB : NB;  // highest VRR row needed
+  R g[NT + 1][NK + 1];
+  g[0][0] = g00;
+  if (NT > 0) {
+    g[1 < NT + 1 ? 1 : 0][0] = c00 * g00;
+#pragma unroll
+    for (int n = 1; n < NT; ++n) g[n + 1][0] = c00 * g[n][0] + R(n) * b10 * g[n - 1][0];
+  }
+#pragma unroll
+  for (int m = 0; m < NK; ++m) {
+    g[0][m + 1] = (m > 0) ? c0p * g[0][m] + R(m) * b01 * g[0][m > 0 ? m - 1 : 0] : c0p * g[0][m];
+#pragma unroll
+    for (int n = 1; n <= NT; ++n) {
+      R v = c0p * g[n][m] + R(n) * b00 * g[n - 1][m];
+      if (m > 0) v += R(m) * b01 * g[n][m > 0 ? m - 1 : 0];
+      g[n][m + 1] = v;
+    }
+  }
+  R h[NT + 1][IB + 1][NK + 1];
+#pragma unroll
+  for (int a = A; a <= NT; ++a)
+#pragma unroll
+    for (int m = 0; m <= NK; ++m) h[a][0][m] = g[a][m];
+#pragma unroll
+  for (int b = 1; b <= IB; ++b)
+#pragma unroll
+    for (int a = A; a + b <= NT; ++a)
+#pragma unroll
+      for (int m = 0; m <= NK; ++m) h[a][b][m] = h[a + 1][b - 1][m] + ab * h[a][b - 1][m];
+#pragma unroll
+  for (int b = 0; b <= IB; ++b) {
+    if (A + b > NB) continue;
+    R k[NK + 1][ID + 1];
+#pragma unroll
+    for (int c = 0; c <= NK; ++c) k[c][0] = h[A][b][c];
+#pragma unroll
+    for (int d = 1; d <= ID; ++d)
+#pragma unroll
+      for (int c = 0; c + d <= NK; ++c) k[c][d] = k[c + 1][d - 1] + cd * k[c][d - 1];
+#pragma unroll
+    for (int c = 0; c <= IC; ++c)
+#pragma unroll
+      for (int d = 0; d <= ID; ++d)
+        if (c + d <= NK) I[((A * (IB + 1) + b) * (IC + 1) + c) * (ID + 1) + d] = k[c][d];
+  }
+}
+
 template <int LA, int LB, int LC, int LD>
 struct Cls {
   static constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
@@ -259,91 +314,100 @@ __global__ void __launch_bounds__(128) jk_kernel(JKArgs args) {
       for (int i = 0; i < C::NCOMP; ++i) acc[i] = group_sum<G>(acc[i]);
     }
     const bool digest = active && sub == 0;
-    // J~_ab += 2f sum_cd (ab|cd) D_cd  -- same bra on every group: warp reduction
-#pragma unroll
-    for (int a = 0; a < C::NA; ++a)
-#pragma unroll
-      for (int b = 0; b < C::NB; ++b) {
-        double v = 0.0;
-        if (digest) {
-#pragma unroll
-          for (int c = 0; c < C::NC; ++c)
-#pragma unroll
-            for (int d = 0; d < C::ND; ++d)
-              v = fma(acc[((a * C::NB + b) * C::NC + c) * C::ND + d], __ldg(D + (kp.oa + c) * n + kp.ob + d), v);
-          v *= 2.0 * f;
-        }
-        v = warp_sum(v);
-        if (lane == 0) atomicAdd((args.J + mb) + (bp.oa + a) * n + bp.ob + b, v);
-      }
-    if (!digest) continue;
-    // J~_cd += 2f sum_ab (ab|cd) D_ab
-    {
-      double dab[C::NA * C::NB];
+    // every density of the call (nset > 1: response densities) is digested
+    // with the same integrals
+    for (int s = 0; s < args.nset; ++s) {
+      const double* __restrict__ Dm = D + s * args.set_stride;
+      double* Jm = args.J + mb + s * args.set_stride;
+      double* Km = DO_K ? args.K + mb + s * args.set_stride : nullptr;
+      // J~_ab += 2f sum_cd (ab|cd) D_cd  -- same bra on every group: warp reduction
 #pragma unroll
       for (int a = 0; a < C::NA; ++a)
 #pragma unroll
-        for (int b = 0; b < C::NB; ++b) dab[a * C::NB + b] = __ldg(D + (bp.oa + a) * n + bp.ob + b);
+        for (int b = 0; b < C::NB; ++b) {
+          double v = 0.0;
+          if (digest) {
 #pragma unroll
-      for (int c = 0; c < C::NC; ++c)
+            for (int c = 0; c < C::NC; ++c)
+#pragma unroll
+              for (int d = 0; d < C::ND; ++d)
+                v = fma(acc[((a * C::NB + b) * C::NC + c) * C::ND + d], __ldg(Dm + (kp.oa + c) * n + kp.ob + d), v);
+            v *= 2.0 * f;
+          }
+          v = warp_sum(v);
+          if (lane == 0) atomicAdd(Jm + (bp.oa + a) * n + bp.ob + b, v);
+        }
+      if (digest) {
+      // J~_cd += 2f sum_ab (ab|cd) D_ab
+      {
+        double dab[C::NA * C::NB];
+#pragma unroll
+        for (int a = 0; a < C::NA; ++a)
+#pragma unroll
+          for (int b = 0; b < C::NB; ++b) dab[a * C::NB + b] = __ldg(Dm + (bp.oa + a) * n + bp.ob + b);
+#pragma unroll
+        for (int c = 0; c < C::NC; ++c)
+#pragma unroll
+          for (int d = 0; d < C::ND; ++d) {
+            double v = 0.0;
+#pragma unroll
+            for (int ab = 0; ab < C::NA * C::NB; ++ab) v = fma(acc[(ab * C::NC + c) * C::ND + d], dab[ab], v);
+            atomicAdd(Jm + (kp.oa + c) * n + kp.ob + d, 2.0 * f * v);
+          }
+      }
+      if constexpr (DO_K) {
+      // K~_ac += f sum_bd I D_bd ; K~_bc += f sum_ad I D_ad ; K~_ad += f sum_bc I D_bc ; K~_bd += f sum_ac I D_ac
+#pragma unroll
+      for (int a = 0; a < C::NA; ++a)
+#pragma unroll
+        for (int c = 0; c < C::NC; ++c) {
+          double v = 0.0;
+#pragma unroll
+          for (int b = 0; b < C::NB; ++b)
+#pragma unroll
+            for (int d = 0; d < C::ND; ++d)
+              v = fma(acc[((a * C::NB + b) * C::NC + c) * C::ND + d], __ldg(Dm + (bp.ob + b) * n + kp.ob + d), v);
+          atomicAdd(Km + (bp.oa + a) * n + kp.oa + c, f * v);
+        }
+#pragma unroll
+      for (int b = 0; b < C::NB; ++b)
+#pragma unroll
+        for (int c = 0; c < C::NC; ++c) {
+          double v = 0.0;
+#pragma unroll
+          for (int a = 0; a < C::NA; ++a)
+#pragma unroll
+            for (int d = 0; d < C::ND; ++d)
+              v = fma(acc[((a * C::NB + b) * C::NC + c) * C::ND + d], __ldg(Dm + (bp.oa + a) * n + kp.ob + d), v);
+          atomicAdd(Km + (bp.ob + b) * n + kp.oa + c, f * v);
+        }
+#pragma unroll
+      for (int a = 0; a < C::NA; ++a)
 #pragma unroll
         for (int d = 0; d < C::ND; ++d) {
           double v = 0.0;
 #pragma unroll
-          for (int ab = 0; ab < C::NA * C::NB; ++ab) v = fma(acc[(ab * C::NC + c) * C::ND + d], dab[ab], v);
-          atomicAdd((args.J + mb) + (kp.oa + c) * n + kp.ob + d, 2.0 * f * v);
+          for (int b = 0; b < C::NB; ++b)
+#pragma unroll
+            for (int c = 0; c < C::NC; ++c)
+              v = fma(acc[((a * C::NB + b) * C::NC + c) * C::ND + d], __ldg(Dm + (bp.ob + b) * n + kp.oa + c), v);
+          atomicAdd(Km + (bp.oa + a) * n + kp.ob + d, f * v);
         }
+#pragma unroll
+      for (int b = 0; b < C::NB; ++b)
+#pragma unroll
+        for (int d = 0; d < C::ND; ++d) {
+          double v = 0.0;
+#pragma unroll
+          for (int a = 0; a < C::NA; ++a)
+#pragma unroll
+            for (int c = 0; c < C::NC; ++c)
+              v = fma(acc[((a * C::NB + b) * C::NC + c) * C::ND + d], __ldg(Dm + (bp.oa + a) * n + kp.oa + c), v);
+          atomicAdd(Km + (bp.ob + b) * n + kp.ob + d, f * v);
+        }
+      }
     }
-    if (!DO_K) continue;
-    // K~_ac += f sum_bd I D_bd ; K~_bc += f sum_ad I D_ad ; K~_ad += f sum_bc I D_bc ; K~_bd += f sum_ac I D_ac
-#pragma unroll
-    for (int a = 0; a < C::NA; ++a)
-#pragma unroll
-      for (int c = 0; c < C::NC; ++c) {
-        double v = 0.0;
-#pragma unroll
-        for (int b = 0; b < C::NB; ++b)
-#pragma unroll
-          for (int d = 0; d < C::ND; ++d)
-            v = fma(acc[((a * C::NB + b) * C::NC + c) * C::ND + d], __ldg(D + (bp.ob + b) * n + kp.ob + d), v);
-        atomicAdd((args.K + mb) + (bp.oa + a) * n + kp.oa + c, f * v);
-      }
-#pragma unroll
-    for (int b = 0; b < C::NB; ++b)
-#pragma unroll
-      for (int c = 0; c < C::NC; ++c) {
-        double v = 0.0;
-#pragma unroll
-        for (int a = 0; a < C::NA; ++a)
-#pragma unroll
-          for (int d = 0; d < C::ND; ++d)
-            v = fma(acc[((a * C::NB + b) * C::NC + c) * C::ND + d], __ldg(D + (bp.oa + a) * n + kp.ob + d), v);
-        atomicAdd((args.K + mb) + (bp.ob + b) * n + kp.oa + c, f * v);
-      }
-#pragma unroll
-    for (int a = 0; a < C::NA; ++a)
-#pragma unroll
-      for (int d = 0; d < C::ND; ++d) {
-        double v = 0.0;
-#pragma unroll
-        for (int b = 0; b < C::NB; ++b)
-#pragma unroll
-          for (int c = 0; c < C::NC; ++c)
-            v = fma(acc[((a * C::NB + b) * C::NC + c) * C::ND + d], __ldg(D + (bp.ob + b) * n + kp.oa + c), v);
-        atomicAdd((args.K + mb) + (bp.oa + a) * n + kp.ob + d, f * v);
-      }
-#pragma unroll
-    for (int b = 0; b < C::NB; ++b)
-#pragma unroll
-      for (int d = 0; d < C::ND; ++d) {
-        double v = 0.0;
-#pragma unroll
-        for (int a = 0; a < C::NA; ++a)
-#pragma unroll
-          for (int c = 0; c < C::NC; ++c)
-            v = fma(acc[((a * C::NB + b) * C::NC + c) * C::ND + d], __ldg(D + (bp.oa + a) * n + kp.oa + c), v);
-        atomicAdd((args.K + mb) + (bp.ob + b) * n + kp.ob + d, f * v);
-      }
+    }
   }
   }  // task loop
 }
@@ -413,7 +477,16 @@ __global__ void __launch_bounds__(128) store_kernel(StoreArgs args) {
 
 // ---------------------------------------------------------------------------
 // Two-electron gradient (eri_gradient_fused, scf/gradient.rs:1430-1640).
-template <typename R, int LA, int LB, int LC, int LD, int G>
+// WSH: the D x D weights of each lane's quartet live in shared memory (one
+// column of NCOMP per thread, read back one component at a time) instead of
+// NCOMP registers, which leaves the registers to the extended tables of the
+// mid-size classes (G = 1 only).
+template <int LA, int LB, int LC, int LD>
+__host__ __device__ constexpr int grad_wsh_doubles() {
+  return 128 * ncart(LA) * ncart(LB) * ncart(LC) * ncart(LD);
+}
+
+template <typename R, int LA, int LB, int LC, int LD, int G, bool WSH = false>
 __global__ void __launch_bounds__(128, (LA + LB + LC + LD <= 1) ? 4 : 1) grad_kernel(GradArgs args) {
   using C = Cls<LA, LB, LC, LD>;
   // tables extended by one on A, B, C; the D derivative follows from
@@ -424,11 +497,15 @@ __global__ void __launch_bounds__(128, (LA + LB + LC + LD <= 1) ? 4 : 1) grad_ke
   constexpr int NR = (LA + LB + LC + LD + 2) / 2 + 1;
   constexpr int NG = 32 / G;
   constexpr bool F32 = sizeof(R) == 4;
+  static_assert(!WSH || G == 1, "shared weights are per thread");
   extern __shared__ double rtab[];
   rys_stage_table<NR>(rtab);
+  // weights of this thread's quartet: Wsh[c * 128] (WSH), as R
+  R* Wsh = reinterpret_cast<R*>(rtab + rys_tab_doubles<NR>()) + threadIdx.x;
+  const volatile R* Wv = Wsh;
   // per-block gradient accumulator: many quartets hit the same few atoms, so
   // global atomics would serialise; one flush per block at the end instead
-  double* gacc = rtab + rys_tab_doubles<NR>();
+  double* gacc = rtab + rys_tab_doubles<NR>() + (WSH ? grad_wsh_doubles<LA, LB, LC, LD>() * sizeof(R) / 8 : 0);
   if (args.gsmem)
     for (int i = threadIdx.x; i < 3 * args.natoms; i += blockDim.x) gacc[i] = 0.0;
   __syncthreads();
@@ -466,7 +543,7 @@ __global__ void __launch_bounds__(128, (LA + LB + LC + LD <= 1) ? 4 : 1) grad_ke
     if (active) {
       const bool kl_same = kp.sa == kp.sb;
       const bool bk_same = task.diag && kpos == task.bra_pos;
-      R W[C::NCOMP];
+      R W[WSH ? 1 : C::NCOMP];
 #pragma unroll
       for (int a = 0; a < C::NA; ++a)
 #pragma unroll
@@ -493,7 +570,10 @@ __global__ void __launch_bounds__(128, (LA + LB + LC + LD <= 1) ? 4 : 1) grad_ke
               // D is angular-scaled: t = w_ref * (ang_a ang_b ang_c ang_d); the
               // |w| < 1e-15 skip applies to the reference weight w_ref
               const double angp = ang_factor(LA, a) * ang_factor(LB, b) * ang_factor(LC, c) * ang_factor(LD, d);
-              W[((a * C::NB + b) * C::NC + c) * C::ND + d] = R((fabs(t / angp) < 1e-15) ? 0.0 : t);
+              const R wt = R((fabs(t / angp) < 1e-15) ? 0.0 : t);
+              const int o = ((a * C::NB + b) * C::NC + c) * C::ND + d;
+              if constexpr (WSH) Wsh[o * 128] = wt;
+              else W[o] = wt;
             }
       const double CD[3] = {kp.A[0] - kp.B[0], kp.A[1] - kp.B[1], kp.A[2] - kp.B[2]};
       const int nitems = bp.np * kp.np;
@@ -521,7 +601,8 @@ __global__ void __launch_bounds__(128, (LA + LB + LC + LD <= 1) ? 4 : 1) grad_ke
         const R a2 = R(2.0 * b.aa), b2 = R(2.0 * (b.p - b.aa)), c2 = R(2.0 * k.aa);
         // FP32 share: this primitive quartet's derivatives in R, then added to the FP64 sums
         R pA[3] = {0, 0, 0}, pB[3] = {0, 0, 0}, pC[3] = {0, 0, 0};
-#pragma unroll
+        // WSH (mid-size classes): one root's tables live at a time
+#pragma unroll (WSH ? 1 : NR)
         for (int r = 0; r < NR; ++r) {
           const double t2 = rt[r];
           // rys_coefficients.rs:94-180 with u2 (p+q) + pq = pq / (1 - t^2):
@@ -543,7 +624,8 @@ __global__ void __launch_bounds__(128, (LA + LB + LC + LD <= 1) ? 4 : 1) grad_ke
               for (int c = 0; c < C::NC; ++c)
 #pragma unroll
                 for (int d = 0; d < C::ND; ++d) {
-                  const R w = W[((a * C::NB + bb) * C::NC + c) * C::ND + d];
+                  const int wo = ((a * C::NB + bb) * C::NC + c) * C::ND + d;
+                  const R w = WSH ? Wv[wo * 128] : W[WSH ? 0 : wo];
                   R reg[3], dA[3], dB[3], dC[3];
 #pragma unroll
                   for (int ax = 0; ax < 3; ++ax) {

@@ -12,6 +12,7 @@
 
 #include "../../include/iqcp.h"
 #include "engine.cuh"
+#include "internal.h"
 
 #include "basis_tables.inc"
 
@@ -99,6 +100,15 @@ struct iqcp_ctx {
   int launches_total = 0;       // every kernel of the last call
   // surviving primitive quartets per task range (counted on first request)
   std::vector<long long> prim_quartets;
+  // multi-density J/K: scaled densities and accumulators of nset densities
+  // (grown on demand), and host-call staging of the inputs and outputs
+  double* d_multi = nullptr;
+  long long multi_cap = 0;      // doubles
+  double* d_multi_io = nullptr;
+  long long multi_io_cap = 0;   // doubles
+  // host copies of the atoms (nuclear repulsion of the batched SCF)
+  std::vector<int> atom_z;
+  std::vector<double> atom_xyz;
 };
 
 namespace {
@@ -267,6 +277,8 @@ JKArgs jk_args(const iqcp_ctx* ctx, const TaskRange& r, const double* Ds, double
   a.next_task = counter;
   a.mol_base = ctx->d_mol_base;
   a.mol_n = ctx->d_mol_n;
+  a.nset = 1;
+  a.set_stride = 0;
   return a;
 }
 
@@ -396,6 +408,20 @@ int finish_stats(iqcp_ctx* ctx) {
 }
 
 }  // namespace
+
+// Accessors for the other translation units of the library (internal.h).
+namespace iqcp {
+cudaStream_t ctx_stream(const iqcp_ctx* c) { return c->stream; }
+int ctx_fail(iqcp_ctx* c, int code, const char* msg) { return fail(c, code, msg); }
+int ctx_device(const iqcp_ctx* c) { return c->device; }
+int ctx_n_mol(const iqcp_ctx* c) { return c->n_mol; }
+const Packing& ctx_packing(const iqcp_ctx* c) { return c->pack; }
+const std::vector<long long>& ctx_mol_base(const iqcp_ctx* c) { return c->mol_base; }
+const std::vector<int>& ctx_mol_nbf(const iqcp_ctx* c) { return c->mol_nbf; }
+const std::vector<int>& ctx_mol_atom0(const iqcp_ctx* c) { return c->mol_atom0; }
+const std::vector<int>& ctx_atom_z(const iqcp_ctx* c) { return c->atom_z; }
+const std::vector<double>& ctx_atom_xyz(const iqcp_ctx* c) { return c->atom_xyz; }
+}  // namespace iqcp
 
 extern "C" {
 
@@ -558,6 +584,8 @@ static int create_batch(int nmol, const iqcp_basis_desc* descs, const iqcp_optio
   }
   ctx->mol_base.push_back(base);
   ctx->mol_atom0.push_back(ctx->n_atoms);
+  ctx->atom_z = bz;
+  ctx->atom_xyz = bxyz;
   ctx->mol_shell0.push_back(ctx->n_shells);
   ctx->packed = base;
   ctx->n_prims = (int)bex.size();
@@ -700,6 +728,8 @@ void iqcp_destroy(iqcp_ctx* ctx) {
   cudaFree(ctx->d_mol_bf0);
   cudaFree(ctx->d_counters);
   cudaFree(ctx->d_fp32);
+  cudaFree(ctx->d_multi);
+  cudaFree(ctx->d_multi_io);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
@@ -858,6 +888,106 @@ int iqcp_fock(iqcp_ctx* ctx, const double* H, const double* D, double k_scale, d
   rc = iqcp_fock_device(ctx, ctx->d_io[1], ctx->d_io[0], k_scale, ctx->d_io[2]);
   if (rc) return rc;
   CK(cudaMemcpyAsync(F, ctx->d_io[2], bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return IQCP_OK;
+}
+
+// Grow a device buffer to at least `need` doubles (contents are not kept).
+static int grow(iqcp_ctx* ctx, double** buf, long long* cap, long long need) {
+  if (*cap >= need) return IQCP_OK;
+  if (*buf) CK(cudaFree(*buf));
+  *buf = nullptr;
+  *cap = 0;
+  if (cudaMalloc(buf, sizeof(double) * (size_t)need) != cudaSuccess)
+    return fail(ctx, IQCP_ERR_NOMEM, "device buffer of " + std::to_string(need) + " doubles");
+  *cap = need;
+  return IQCP_OK;
+}
+
+int iqcp_jk_multi_device(iqcp_ctx* ctx, int nset, const double* dD, double* dJ, double* dK) {
+  if (!ctx || nset < 1 || !dD || !dJ) return IQCP_ERR_ARG;
+  int rc = ensure_device(ctx);
+  if (rc) return rc;
+  const long long nn = ctx->packed;
+  rc = grow(ctx, &ctx->d_multi, &ctx->multi_cap, 3 * nn * nset);
+  if (rc) return rc;
+  double* Ds = ctx->d_multi;
+  double* Jt = Ds + nn * nset;
+  double* Kt = Jt + nn * nset;
+  const bool want_k = dK != nullptr;
+  ctx->launches_total = 0;
+  for (int s = 0; s < nset; ++s)
+    CK(launch_scale_density(dD + s * nn, ctx->d_ang, ctx->pack, Ds + s * nn, ctx->stream));
+  ctx->launches_total += nset;
+  ctx->mixed_call = false;  // response densities: FP64 quadrature
+  CK(cudaMemsetAsync(Jt, 0, sizeof(double) * nn * nset, ctx->stream));
+  if (want_k) CK(cudaMemsetAsync(Kt, 0, sizeof(double) * nn * nset, ctx->stream));
+  rc = run_ranges(ctx, 0, [&](const TaskRange& r, int pass, int* counter) {
+    JKArgs a = jk_args(ctx, r, Ds, Jt, want_k ? Kt : nullptr, r.mode[0], pass, counter);
+    a.nset = nset;
+    a.set_stride = nn;
+    return launch_jk(r.X, r.Y, a, ctx->stream);
+  });
+  if (rc) return rc;
+  for (int s = 0; s < nset; ++s) {
+    CK(launch_symmetrize(Jt + s * nn, ctx->d_ang, ctx->pack, dJ + s * nn, ctx->stream));
+    if (want_k) CK(launch_symmetrize(Kt + s * nn, ctx->d_ang, ctx->pack, dK + s * nn, ctx->stream));
+  }
+  ctx->launches_total += nset * (want_k ? 2 : 1);
+  return finish_stats(ctx);
+}
+
+int iqcp_jk_multi(iqcp_ctx* ctx, int nset, const double* D, double* J, double* K) {
+  if (!ctx || nset < 1 || !D || !J) return IQCP_ERR_ARG;
+  int rc = ensure_device(ctx);
+  if (rc) return rc;
+  const long long nn = ctx->packed;
+  rc = grow(ctx, &ctx->d_multi_io, &ctx->multi_io_cap, 3 * nn * nset);
+  if (rc) return rc;
+  double* dD = ctx->d_multi_io;
+  double* dJ = dD + nn * nset;
+  double* dK = dJ + nn * nset;
+  const size_t bytes = sizeof(double) * (size_t)(nn * nset);
+  CK(cudaMemcpyAsync(dD, D, bytes, cudaMemcpyHostToDevice, ctx->stream));
+  rc = iqcp_jk_multi_device(ctx, nset, dD, dJ, K ? dK : nullptr);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(J, dJ, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  if (K) CK(cudaMemcpyAsync(K, dK, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return IQCP_OK;
+}
+
+// G = J - 1/2 k_scale K and F = H + G, element by element over the packed matrices.
+static __global__ void fock_parts_kernel(const double* __restrict__ H, const double* __restrict__ J,
+                                  const double* __restrict__ K, double kscale, long long n, double* __restrict__ G,
+                                  double* __restrict__ F) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double g = J[i] - 0.5 * kscale * K[i];
+    if (G) G[i] = g;
+    if (F) F[i] = H[i] + g;
+  }
+}
+
+int iqcp_fock_decomposition(iqcp_ctx* ctx, const double* H, const double* D, double k_scale, double* J, double* K,
+                            double* G, double* F) {
+  if (!ctx || !D || (F && !H)) return IQCP_ERR_ARG;
+  int rc = ensure_device(ctx);
+  if (rc) return rc;
+  const long long nn = ctx->packed;
+  const size_t bytes = sizeof(double) * (size_t)nn;
+  // staging: D, then H (after the build) in io[0]; J io[1], K io[2], G io[3]; F over H
+  CK(cudaMemcpyAsync(ctx->d_io[0], D, bytes, cudaMemcpyHostToDevice, ctx->stream));
+  rc = iqcp_jk_device(ctx, ctx->d_io[0], ctx->d_io[1], ctx->d_io[2]);
+  if (rc) return rc;
+  if (H) CK(cudaMemcpyAsync(ctx->d_io[0], H, bytes, cudaMemcpyHostToDevice, ctx->stream));
+  const int blocks = (int)std::min<long long>((nn + 255) / 256, 4096);
+  fock_parts_kernel<<<blocks, 256, 0, ctx->stream>>>(H ? ctx->d_io[0] : nullptr, ctx->d_io[1], ctx->d_io[2],
+                                                      k_scale, nn, ctx->d_io[3], H ? ctx->d_io[0] : nullptr);
+  CK(cudaGetLastError());
+  if (J) CK(cudaMemcpyAsync(J, ctx->d_io[1], bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  if (K) CK(cudaMemcpyAsync(K, ctx->d_io[2], bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  if (G) CK(cudaMemcpyAsync(G, ctx->d_io[3], bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  if (F) CK(cudaMemcpyAsync(F, ctx->d_io[0], bytes, cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
   return IQCP_OK;
 }

@@ -1,14 +1,23 @@
-"""Batched device RHF (one CUDA graph per iteration) against the per-geometry
-host driver: converged energies within 1e-8 Ha and RHF gradients within
-1e-6 Ha/bohr of rhf_scf + rhf_gradient run geometry by geometry."""
+"""Batched device RHF through the C ABI (iqcp_batch_scf: one CUDA graph per
+iteration, DIIS and canonical purification on the device, no host linear
+algebra) against the per-geometry host driver run geometry by geometry with
+the same Fock builder: converged energies within 1 nHa, densities within
+1e-6 and RHF gradients within 1e-7 Ha/bohr; and against the oracle's
+converged energy of the 40-atom workload."""
+import json
+import os
+
 import numpy as np
 import pytest
 
+from conftest import GOLDEN
 from iqcp_b200 import BasisSet, FockEngine
+from iqcp_b200.batch_scf import BatchRHF
 from iqcp_b200.molecules import REFERENCE_MOLECULES, batch_geometries
 from iqcp_b200.scf import energy_weighted_density, rhf_scf
 
 pytestmark = pytest.mark.gpu
+TIGHT = dict(e_tol=1e-11, d_tol=1e-9, err_tol=1e-8, max_iter=120)
 
 
 @pytest.fixture(scope="module")
@@ -26,44 +35,61 @@ def reference(bases):
     for b in bases:
         with FockEngine(b) as eng:
             S, T, V = eng.one_electron()
-            res = rhf_scf(S, T + V, b.nuclear_repulsion(), b.n_electrons // 2, eng.build_fock, e_tol=1e-11,
-                          d_tol=1e-9)
+            res = rhf_scf(S, T + V, b.nuclear_repulsion(), b.n_electrons // 2, eng.build_fock, e_tol=1e-12,
+                          d_tol=1e-10)
             W = energy_weighted_density(res.mo_coefficients, res.mo_energies, res.n_occ)
             ref.append((res.energy, eng.rhf_gradient(res.density, W), res.density))
     return ref
 
 
-@pytest.mark.parametrize("use_graph", [True, False])
-def test_batch_rhf_energies_and_gradients(bases, reference, use_graph):
-    from iqcp_b200.batch_scf import BatchRHF
-
-    scf = BatchRHF(bases, n_groups=3)
-    res = scf.run(e_tol=1e-10, d_tol=1e-8, err_tol=1e-7, use_graph=use_graph)
+def test_batch_scf_energies_densities_gradients(bases, reference):
+    scf = BatchRHF(bases)
+    res = scf.run(**TIGHT)
     assert res.converged.all(), res.__dict__
-    assert res.idempotency.max() < 1e-10
     grads = scf.gradients()
     dens = scf.densities()
     for (e_ref, g_ref, d_ref), e, g, d in zip(reference, res.energies, grads, dens):
-        assert abs(e - e_ref) < 1e-8, (e, e_ref)
-        assert np.abs(d - d_ref).max() < 1e-5
-        assert np.abs(g - g_ref).max() < 1e-6
+        assert abs(e - e_ref) < 1e-9, (e, e_ref)
+        assert np.abs(d - d_ref).max() < 1e-6
+        assert np.abs(g - g_ref).max() < 1e-7
+    scf.close()
 
 
-def test_batch_rhf_handoff(bases, reference):
-    """Hand-off of the unconverged geometries to a smaller batch after a few
-    iterations reaches the same energies, densities and gradients."""
-    from iqcp_b200.batch_scf import BatchRHF
+def test_batch_scf_core_guess_is_aufbau(bases):
+    """The purified core guess equals the eigen-decomposition one (scf/mod.rs:1379-1389)."""
+    scf = BatchRHF(bases[:3])
+    D = scf.eng.unpack(scf.core_guess())
+    for b, Dg in zip(bases[:3], D):
+        with FockEngine(b) as eng:
+            S, T, V = eng.one_electron()
+        w, U = np.linalg.eigh(S)
+        X = (U / np.sqrt(w)) @ U.T
+        _, C = np.linalg.eigh(X.T @ (T + V) @ X)
+        C = X @ C[:, :b.n_electrons // 2]
+        assert np.abs(Dg - 2.0 * C @ C.T).max() < 1e-8
+    scf.close()
 
-    scf = BatchRHF(bases, n_groups=3)
-    res = scf.run(e_tol=1e-10, d_tol=1e-8, err_tol=1e-7, handoff=0.3, handoff_after=3)
-    assert res.converged.all(), res.__dict__
-    grads = scf.gradients()
-    # the device calls and the torch steps between them share one stream: a
-    # second evaluation agrees to rounding
-    again = scf.gradients()
-    assert max(np.abs(a - b).max() for a, b in zip(grads, again)) < 1e-10
-    dens = scf.densities()
-    for (e_ref, g_ref, d_ref), e, g, d in zip(reference, res.energies, grads, dens):
-        assert abs(e - e_ref) < 1e-8, (e, e_ref)
-        assert np.abs(d - d_ref).max() < 1e-5
-        assert np.abs(g - g_ref).max() < 1e-6
+
+def test_batch_scf_single_context_and_start_density(bases, reference):
+    """A one-geometry batch started from a converged density stays there."""
+    scf = BatchRHF(bases[:1])
+    res = scf.run(D0=[reference[0][2]], **TIGHT)
+    assert res.converged.all() and res.iterations <= 5
+    assert abs(res.energies[0] - reference[0][0]) < 1e-9
+    scf.close()
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(GOLDEN, "config_c2.npz")), reason="fixture not generated")
+def test_batch_scf_c2_oracle_energy():
+    """The 40-atom RHF/6-31G* workload from the core guess converges to the
+    oracle's energy within 1 nHa."""
+    f = np.load(os.path.join(GOLDEN, "config_c2.npz"))
+    meta = json.loads(str(f["meta"]))
+    atoms = [(int(z), tuple(x)) for z, x in zip(f["z"], f["xyz"])]
+    b = BasisSet.build(atoms, meta["basis"])
+    scf = BatchRHF([b])
+    res = scf.run(**TIGHT)
+    assert res.converged.all()
+    assert abs(res.energies[0] - meta["energy"]) < 1e-9, (res.energies[0], meta["energy"])
+    assert np.abs(scf.gradients()[0] - f["grad_rhf"]).max() < 1e-7
+    scf.close()

@@ -1,6 +1,8 @@
 """Every quartet-kernel variant the autotuner can choose gives the oracle's
 J/K and gradient: 0 one quartet per thread, 1 one warp per quartet
-(shared-memory tables), 2 / 3 eight / thirty-two lanes per quartet."""
+(shared-memory tables), 2 / 3 eight / thirty-two lanes per quartet for J/K;
+for gradients 2 is one quartet per thread with its weights in shared memory
+and 3 thirty-two lanes over (primitive quartet, root) items."""
 import numpy as np
 import pytest
 

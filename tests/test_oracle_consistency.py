@@ -66,3 +66,26 @@ def test_rhf_gradient_vs_finite_difference(oracle_mod):
             e.append(_scf(oracle_mod, BasisSet.build([(z, tuple(x)) for z, x in at], "6-31g*")).energy)
         fd = (e[0] - e[1]) / (2 * h)
         assert abs(fd - g[atom, d]) < 1e-7, (atom, d, fd, g[atom, d])
+
+
+def test_stride_phases_partition_the_workload(oracle_mod):
+    """The benchmark's reference arm times the oracle on bra-pair phases
+    P % K == k, k = 0..K-1: together they are exactly one full J/K build and
+    one full gradient."""
+    from iqcp_b200.molecules import REFERENCE_MOLECULES
+    from oracle.basis import build_basis
+    b = build_basis(REFERENCE_MOLECULES["H2O"], "6-31g*")
+    rng = np.random.default_rng(4)
+    A = rng.normal(size=(b.n_basis, b.n_basis)) * 0.1
+    D = A + A.T
+    J, K, _ = oracle_mod.jk_direct(b, D)
+    g, _ = oracle_mod.eri_gradient(b, D, 1.0)
+    Js, Ks, gs = np.zeros_like(J), np.zeros_like(K), np.zeros_like(g)
+    for k in range(3):
+        Jk, Kk, _ = oracle_mod.jk_direct(b, D, 3, k)
+        gk, _ = oracle_mod.eri_gradient(b, D, 1.0, 3, k)
+        Js += Jk
+        Ks += Kk
+        gs += gk
+    assert np.abs(Js - J).max() < 1e-12 and np.abs(Ks - K).max() < 1e-12
+    assert np.abs(gs - g).max() < 1e-12
