@@ -190,6 +190,19 @@ int iqcp_jk_multi(iqcp_ctx* ctx, int nset, const double* D, double* J, double* K
 int iqcp_jk_multi_device(iqcp_ctx* ctx, int nset, const double* d_D, double* d_J, double* d_K);
 
 /*
+ * J and K in the real spherical-harmonic basis (single-geometry contexts):
+ * D, J, K are nsph x nsph, nsph = iqcp_nbf_spherical(ctx) = sum over shells of
+ * 2l + 1, functions shell by shell with m = -l..l (d: d-2, d-1, d0, d+1, d+2).
+ * The reference's spherical path transforms each Cartesian ERI block with
+ * EriSphericalTransform (integrals/spherical.rs:390-470, coefficients
+ * CART2SPH_D :71) and digests the transformed ERIs; here J_sph =
+ * C^T J_cart[C D C^T] C with the same coefficients (C[cart][sph]), which is
+ * the same sum.  K may be NULL.
+ */
+int iqcp_nbf_spherical(iqcp_ctx* ctx);
+int iqcp_jk_spherical(iqcp_ctx* ctx, const double* D, double* J, double* K);
+
+/*
  * The four matrices of compute_fock_decomposition (scf/fock.rs:104-179), host
  * buffers: J, K, G = J - 1/2 k_scale K and F = H + G (k_scale = 1 for RHF).
  * Any output may be NULL; H may be NULL when F is.

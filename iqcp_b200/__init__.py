@@ -118,6 +118,8 @@ EXPORTS = {
                                             ctypes.c_void_p]),
     "iqcp_fock_decomposition": (ctypes.c_int, [ctypes.c_void_p, _c_dbl_p, _c_dbl_p, ctypes.c_double, _c_dbl_p,
                                                _c_dbl_p, _c_dbl_p, _c_dbl_p]),
+    "iqcp_nbf_spherical": (ctypes.c_int, [ctypes.c_void_p]),
+    "iqcp_jk_spherical": (ctypes.c_int, [ctypes.c_void_p, _c_dbl_p, _c_dbl_p, _c_dbl_p]),
     "iqcp_scf_default_options": (None, [ctypes.POINTER(ScfOptions)]),
     "iqcp_batch_scf": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ScfOptions), _c_dbl_p, _c_dbl_p, _c_int_p,
                                       _c_int_p, _c_dbl_p, _c_dbl_p]),
@@ -299,6 +301,18 @@ class FockEngine:
     def jk_multi_device(self, nset, d_D, d_J, d_K=None):
         self._check(self._lib.iqcp_jk_multi_device(self._h, int(nset), ctypes.c_void_p(d_D), ctypes.c_void_p(d_J),
                                                    ctypes.c_void_p(d_K) if d_K else None))
+
+    def build_jk_spherical(self, D, with_k=True):
+        """J and K in the spherical basis (nsph x nsph, m = -l..l per shell):
+        the reference's use_spherical path (EriSphericalTransform, spherical.rs:390)."""
+        n = self._lib.iqcp_nbf_spherical(self._h)
+        D = np.ascontiguousarray(D, dtype=np.float64)
+        if D.shape != (n, n):
+            raise ValueError("expected a %dx%d matrix" % (n, n))
+        J = np.empty_like(D)
+        K = np.empty_like(D) if with_k else None
+        self._check(self._lib.iqcp_jk_spherical(self._h, _dp(D), _dp(J), _dp(K) if with_k else None))
+        return (J, K) if with_k else J
 
     def fock_decomposition(self, H, D, k_scale=1.0):
         """(J, K, G, F) with G = J - k_scale/2 K, F = H + G: compute_fock_decomposition

@@ -139,7 +139,13 @@ struct JKArgs {
   const int* mol_n;           // per molecule: nbf (row stride of its block)
   int nset;                   // densities digested per quartet (1, or several response densities)
   long long set_stride;       // elements between consecutive densities in D, J and K
+  const int* mol_active;      // per molecule: 0 = skip its tasks (a converged geometry of a batched SCF); may be null
 };
+
+// Tasks of molecules flagged inactive are skipped (the same on every lane).
+__device__ __forceinline__ bool task_inactive(const int* mol_active, int mol) {
+  return mol_active != nullptr && __ldg(mol_active + mol) == 0;
+}
 
 struct StoreArgs {
   const ShellPair* pairs;

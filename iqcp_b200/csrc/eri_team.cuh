@@ -146,6 +146,7 @@ __global__ void __launch_bounds__(128) jk_team_kernel(JKArgs args) {
   for (int warp = next_task(args.next_task, lane); warp < args.ntasks; warp = next_task(args.next_task, lane)) {
   const QuartetTask task = args.tasks[warp];
   const ShellPair bp = args.pairs[task.bra];
+  if (task_inactive(args.mol_active, bp.mol)) continue;
   // this task's molecule block (bra and ket pairs always share a molecule)
   const int n = args.mol_n[bp.mol];
   const long long mb = args.mol_base[bp.mol];

@@ -106,6 +106,15 @@ struct iqcp_ctx {
   long long multi_cap = 0;      // doubles
   double* d_multi_io = nullptr;
   long long multi_io_cap = 0;   // doubles
+  // spherical basis (single geometry): per Cartesian function {sph offset of
+  // its shell, position in the shell, l}, per spherical function {Cartesian
+  // offset of its shell, m index, l}; built on first use
+  int nsph = 0;
+  int* d_cart_info = nullptr;
+  int* d_sph_info = nullptr;
+  // batched SCF: per-molecule flags of the geometries still iterating (device,
+  // owned by the SCF call; null = every molecule)
+  const int* mol_active = nullptr;
   // host copies of the atoms (nuclear repulsion of the batched SCF)
   std::vector<int> atom_z;
   std::vector<double> atom_xyz;
@@ -279,6 +288,7 @@ JKArgs jk_args(const iqcp_ctx* ctx, const TaskRange& r, const double* Ds, double
   a.mol_n = ctx->d_mol_n;
   a.nset = 1;
   a.set_stride = 0;
+  a.mol_active = ctx->mol_active;
   return a;
 }
 
@@ -421,6 +431,7 @@ const std::vector<int>& ctx_mol_nbf(const iqcp_ctx* c) { return c->mol_nbf; }
 const std::vector<int>& ctx_mol_atom0(const iqcp_ctx* c) { return c->mol_atom0; }
 const std::vector<int>& ctx_atom_z(const iqcp_ctx* c) { return c->atom_z; }
 const std::vector<double>& ctx_atom_xyz(const iqcp_ctx* c) { return c->atom_xyz; }
+void ctx_set_mol_active(iqcp_ctx* c, const int* d_flags) { c->mol_active = d_flags; }
 }  // namespace iqcp
 
 extern "C" {
@@ -730,6 +741,8 @@ void iqcp_destroy(iqcp_ctx* ctx) {
   cudaFree(ctx->d_fp32);
   cudaFree(ctx->d_multi);
   cudaFree(ctx->d_multi_io);
+  cudaFree(ctx->d_cart_info);
+  cudaFree(ctx->d_sph_info);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
@@ -988,6 +1001,114 @@ int iqcp_fock_decomposition(iqcp_ctx* ctx, const double* H, const double* D, dou
   if (K) CK(cudaMemcpyAsync(K, ctx->d_io[2], bytes, cudaMemcpyDeviceToHost, ctx->stream));
   if (G) CK(cudaMemcpyAsync(G, ctx->d_io[3], bytes, cudaMemcpyDeviceToHost, ctx->stream));
   if (F) CK(cudaMemcpyAsync(F, ctx->d_io[0], bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return IQCP_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Spherical basis.  Real solid harmonics from Cartesian functions with the
+// coefficients C[cart][sph] the reference uses (CART2SPH_D, integrals/spherical.rs:71,
+// libcint cart2sph): AO_sph = C^T AO_cart per shell; identity for s and p.
+// Both the ERI transform of the reference's spherical path (EriSphericalTransform,
+// spherical.rs:390-470, then J/K from the transformed ERIs) and J/K linearity
+// give J_sph[D_sph] = C^T J_cart[C D_sph C^T] C, likewise K.
+__constant__ double kCart2SphD[6][5] = {
+    {0.0, 0.0, -0.315391565252520002, 0.0, 0.546274215296039535},
+    {1.092548430592079070, 0.0, 0.0, 0.0, 0.0},
+    {0.0, 0.0, 0.0, 1.092548430592079070, 0.0},
+    {0.0, 0.0, -0.315391565252520002, 0.0, -0.546274215296039535},
+    {0.0, 1.092548430592079070, 0.0, 0.0, 0.0},
+    {0.0, 0.0, 0.630783130505040012, 0.0, 0.0}};
+
+__device__ __forceinline__ double cart2sph(int l, int c, int m) {
+  return l == 2 ? kCart2SphD[c][m] : (c == m ? 1.0 : 0.0);
+}
+
+// Dc = C Ds C^T (Cartesian from spherical), element per thread
+static __global__ void sph_to_cart_kernel(int nc, int ns, const int4* __restrict__ cinfo,
+                                          const double* __restrict__ Ds, double* __restrict__ Dc) {
+  const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (e >= (long long)nc * nc) return;
+  const int a = int(e / nc), b = int(e - (long long)a * nc);
+  const int4 ia = cinfo[a], ib = cinfo[b];  // {sph offset, position, l, -}
+  double v = 0.0;
+  for (int i = 0; i < 2 * ia.z + 1; ++i) {
+    const double ca = cart2sph(ia.z, ia.y, i);
+    if (ca == 0.0) continue;
+    for (int j = 0; j < 2 * ib.z + 1; ++j)
+      v = fma(ca * cart2sph(ib.z, ib.y, j), Ds[(long long)(ia.x + i) * ns + ib.x + j], v);
+  }
+  Dc[e] = v;
+}
+
+// Xs = C^T Xc C (spherical from Cartesian), element per thread
+static __global__ void cart_to_sph_kernel(int nc, int ns, const int4* __restrict__ sinfo,
+                                          const double* __restrict__ Xc, double* __restrict__ Xs) {
+  const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (e >= (long long)ns * ns) return;
+  const int i = int(e / ns), j = int(e - (long long)i * ns);
+  const int4 si = sinfo[i], sj = sinfo[j];  // {Cartesian offset, m, l, -}
+  const int na = (si.z + 1) * (si.z + 2) / 2, nb = (sj.z + 1) * (sj.z + 2) / 2;
+  double v = 0.0;
+  for (int a = 0; a < na; ++a) {
+    const double ca = cart2sph(si.z, a, si.y);
+    if (ca == 0.0) continue;
+    for (int b = 0; b < nb; ++b)
+      v = fma(ca * cart2sph(sj.z, b, sj.y), Xc[(long long)(si.x + a) * nc + sj.x + b], v);
+  }
+  Xs[e] = v;
+}
+
+static int spherical_tables(iqcp_ctx* ctx) {
+  if (ctx->d_cart_info) return IQCP_OK;
+  std::vector<int4> ci, si;
+  int os = 0;
+  for (int s = 0; s < ctx->n_shells; ++s) {
+    const int l = ctx->shell_l[s], oc = ctx->shell_off[s];
+    for (int c = 0; c < ncart(l); ++c) ci.push_back(make_int4(os, c, l, 0));
+    for (int m = 0; m < 2 * l + 1; ++m) si.push_back(make_int4(oc, m, l, 0));
+    os += 2 * l + 1;
+  }
+  ctx->nsph = os;
+  CK(cudaMalloc(&ctx->d_cart_info, sizeof(int4) * ci.size()));
+  CK(cudaMalloc(&ctx->d_sph_info, sizeof(int4) * si.size()));
+  CK(cudaMemcpy(ctx->d_cart_info, ci.data(), sizeof(int4) * ci.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(ctx->d_sph_info, si.data(), sizeof(int4) * si.size(), cudaMemcpyHostToDevice));
+  return IQCP_OK;
+}
+
+int iqcp_nbf_spherical(iqcp_ctx* ctx) {
+  if (!ctx) return 0;
+  int n = 0;
+  for (int s = 0; s < ctx->n_shells; ++s) n += 2 * ctx->shell_l[s] + 1;
+  return n;
+}
+
+int iqcp_jk_spherical(iqcp_ctx* ctx, const double* Ds, double* Js, double* Ks) {
+  if (!ctx || !Ds || !Js) return IQCP_ERR_ARG;
+  if (ctx->n_mol != 1) return fail(ctx, IQCP_ERR_ARG, "iqcp_jk_spherical takes single-geometry contexts");
+  int rc = ensure_device(ctx);
+  if (rc) return rc;
+  if ((rc = spherical_tables(ctx))) return rc;
+  const int nc = ctx->nbf, ns = ctx->nsph;
+  const long long ncc = (long long)nc * nc, nss = (long long)ns * ns;
+  const int4* cinfo = reinterpret_cast<const int4*>(ctx->d_cart_info);
+  const int4* sinfo = reinterpret_cast<const int4*>(ctx->d_sph_info);
+  // io[3] <- D_sph; io[0] <- D_cart; J_cart, K_cart in io[1], io[2]; results back through io[3], io[0]
+  CK(cudaMemcpyAsync(ctx->d_io[3], Ds, sizeof(double) * nss, cudaMemcpyHostToDevice, ctx->stream));
+  sph_to_cart_kernel<<<(int)((ncc + 255) / 256), 256, 0, ctx->stream>>>(nc, ns, cinfo, ctx->d_io[3], ctx->d_io[0]);
+  CK(cudaGetLastError());
+  rc = iqcp_jk_device(ctx, ctx->d_io[0], ctx->d_io[1], Ks ? ctx->d_io[2] : nullptr);
+  if (rc) return rc;
+  cart_to_sph_kernel<<<(int)((nss + 255) / 256), 256, 0, ctx->stream>>>(nc, ns, sinfo, ctx->d_io[1], ctx->d_io[3]);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(Js, ctx->d_io[3], sizeof(double) * nss, cudaMemcpyDeviceToHost, ctx->stream));
+  if (Ks) {
+    cart_to_sph_kernel<<<(int)((nss + 255) / 256), 256, 0, ctx->stream>>>(nc, ns, sinfo, ctx->d_io[2],
+                                                                           ctx->d_io[0]);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(Ks, ctx->d_io[0], sizeof(double) * nss, cudaMemcpyDeviceToHost, ctx->stream));
+  }
   CK(cudaStreamSynchronize(ctx->stream));
   return IQCP_OK;
 }

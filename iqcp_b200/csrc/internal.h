@@ -21,4 +21,6 @@ const std::vector<int>& ctx_mol_nbf(const iqcp_ctx* c);
 const std::vector<int>& ctx_mol_atom0(const iqcp_ctx* c);       // n_mol + 1
 const std::vector<int>& ctx_atom_z(const iqcp_ctx* c);
 const std::vector<double>& ctx_atom_xyz(const iqcp_ctx* c);     // 3 per atom, bohr
+// J/K and Fock builds skip the molecules whose flag is 0 (null: none skipped)
+void ctx_set_mol_active(iqcp_ctx* c, const int* d_flags);
 }  // namespace iqcp

@@ -50,15 +50,22 @@ constexpr int kMaxDiis = 16;
 // chunks of 16 staged in shared memory.
 constexpr int GT = 64, GK = 16;
 
+// Molecules whose flag in `active` is 0 (converged geometries of the batched
+// SCF) are skipped by every per-molecule kernel below; active may be null.
+__device__ __forceinline__ bool frozen(const int* __restrict__ active, int m) {
+  return active != nullptr && active[m] == 0;
+}
+
 template <bool TA, bool TB>
 __global__ void __launch_bounds__(256) gemm_packed_kernel(const long long* __restrict__ base,
-                                                          const int* __restrict__ nm, const double* __restrict__ A,
+                                                          const int* __restrict__ nm, const int* __restrict__ active,
+                                                          const double* __restrict__ A,
                                                           const double* __restrict__ B, double* __restrict__ C,
                                                           double alpha, double beta) {
   const int m = blockIdx.z;
   const int n = nm[m];
   const int r0 = blockIdx.y * GT, c0 = blockIdx.x * GT;
-  if (r0 >= n || c0 >= n) return;
+  if (r0 >= n || c0 >= n || frozen(active, m)) return;
   const long long o = base[m];
   const double* Am = A + o;
   const double* Bm = B + o;
@@ -135,11 +142,13 @@ __device__ __forceinline__ double block_max(double v, double* sh) {
 }
 
 // E_m = 1/2 sum D (H + F) + E_nuc_m; dE_m = E_m - E_m(previous).  One block per molecule.
-__global__ void energy_kernel(const long long* __restrict__ base, const double* __restrict__ D,
-                              const double* __restrict__ H, const double* __restrict__ F,
-                              const double* __restrict__ enuc, double* __restrict__ E, double* __restrict__ dE) {
+__global__ void energy_kernel(const long long* __restrict__ base, const int* __restrict__ active,
+                              const double* __restrict__ D, const double* __restrict__ H,
+                              const double* __restrict__ F, const double* __restrict__ enuc, double* __restrict__ E,
+                              double* __restrict__ dE) {
   __shared__ double sh[8];
   const int m = blockIdx.x;
+  if (frozen(active, m)) return;
   double s = 0.0;
   for (long long i = base[m] + threadIdx.x; i < base[m + 1]; i += blockDim.x) s += D[i] * (H[i] + F[i]);
   s = block_sum(s, sh);
@@ -152,8 +161,10 @@ __global__ void energy_kernel(const long long* __restrict__ base, const double* 
 
 // out = T - T^T per molecule block (grid: chunks x molecules)
 __global__ void antisym_kernel(const long long* __restrict__ base, const int* __restrict__ nm,
-                               const double* __restrict__ T, double* __restrict__ out) {
+                               const int* __restrict__ active, const double* __restrict__ T,
+                               double* __restrict__ out) {
   const int m = blockIdx.y, n = nm[m];
+  if (frozen(active, m)) return;
   const long long o = base[m], nn = (long long)n * n;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nn; e += (long long)gridDim.x * blockDim.x) {
     const int i = int(e / n), j = int(e - (long long)i * n);
@@ -173,10 +184,11 @@ __global__ void maxabs_kernel(const long long* __restrict__ base, const double* 
 }
 
 // rms difference sqrt(sum (A - B)^2 / n^2) per molecule; then B = A
-__global__ void rmsdiff_copy_kernel(const long long* __restrict__ base, const double* __restrict__ A,
-                                    double* __restrict__ B, double* __restrict__ out) {
+__global__ void rmsdiff_copy_kernel(const long long* __restrict__ base, const int* __restrict__ active,
+                                    const double* __restrict__ A, double* __restrict__ B, double* __restrict__ out) {
   __shared__ double sh[8];
   const int m = blockIdx.x;
+  if (frozen(active, m)) return;
   double s = 0.0;
   for (long long i = base[m] + threadIdx.x; i < base[m + 1]; i += blockDim.x) {
     const double d = A[i] - B[i];
@@ -255,10 +267,11 @@ __global__ void diis_solve_kernel(int nmol, int K, const int* __restrict__ count
 }
 
 // Fx = sum_k c_k Fbuf[k] per molecule block (grid: chunks x molecules)
-__global__ void diis_extrapolate_kernel(const long long* __restrict__ base, long long total, int K,
-                                        const double* __restrict__ coef, const double* __restrict__ Fbuf,
-                                        double* __restrict__ Fx) {
+__global__ void diis_extrapolate_kernel(const long long* __restrict__ base, const int* __restrict__ active,
+                                        long long total, int K, const double* __restrict__ coef,
+                                        const double* __restrict__ Fbuf, double* __restrict__ Fx) {
   const int m = blockIdx.y;
+  if (frozen(active, m)) return;
   const long long o = base[m], nn = base[m + 1] - o;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nn; e += (long long)gridDim.x * blockDim.x) {
     double v = 0.0;
@@ -276,11 +289,12 @@ __global__ void diis_advance_kernel(int K, int* slot, int* count) {
 // mu = Tr F' / n, lambda = min(ne / (emax - mu), (n - ne) / (mu - emin));
 // P0 = lambda/n (mu I - F') + ne/n I.  One block per molecule.
 __global__ void purify_start_kernel(const long long* __restrict__ base, const int* __restrict__ nm,
-                                    const int* __restrict__ nocc, const double* __restrict__ Fp,
-                                    double* __restrict__ P) {
+                                    const int* __restrict__ active, const int* __restrict__ nocc,
+                                    const double* __restrict__ Fp, double* __restrict__ P) {
   __shared__ double sh[8];
   __shared__ double par[2];
   const int m = blockIdx.x, n = nm[m];
+  if (frozen(active, m)) return;
   const double* F = Fp + base[m];
   double lo = 1e300, hi = -1e300, tr = 0.0;
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
@@ -312,10 +326,12 @@ __global__ void purify_start_kernel(const long long* __restrict__ base, const in
 // Canonical purification, traces of one step: tr[2m] = Tr(P - P2),
 // tr[2m+1] = Tr(P2 - P3).  One block per molecule.
 __global__ void purify_trace_kernel(const long long* __restrict__ base, const int* __restrict__ nm,
-                                    const double* __restrict__ P, const double* __restrict__ P2,
-                                    const double* __restrict__ P3, double* __restrict__ tr) {
+                                    const int* __restrict__ active, const double* __restrict__ P,
+                                    const double* __restrict__ P2, const double* __restrict__ P3,
+                                    double* __restrict__ tr) {
   __shared__ double sh[8];
   const int m = blockIdx.x, n = nm[m];
+  if (frozen(active, m)) return;
   const long long o = base[m];
   double a = 0.0, b = 0.0;
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
@@ -335,10 +351,11 @@ __global__ void purify_trace_kernel(const long long* __restrict__ base, const in
 // c >= 1/2, else ((1 - 2c) P + (1 + c) P2 - P3) / (1 - c).  Once P is
 // idempotent to rounding t1 vanishes and the McWeeny step (c = 1/2) is taken.
 // Grid: chunks x molecules.
-__global__ void purify_update_kernel(const long long* __restrict__ base, const double* __restrict__ tr,
-                                     double* __restrict__ P, const double* __restrict__ P2,
-                                     const double* __restrict__ P3) {
+__global__ void purify_update_kernel(const long long* __restrict__ base, const int* __restrict__ active,
+                                     const double* __restrict__ tr, double* __restrict__ P,
+                                     const double* __restrict__ P2, const double* __restrict__ P3) {
   const int m = blockIdx.y;
+  if (frozen(active, m)) return;
   const long long o = base[m], nn = base[m + 1] - o;
   const double t1 = tr[2 * m], t2 = tr[2 * m + 1];
   const double c = fabs(t1) < 1e-13 ? 0.5 : t2 / t1;
@@ -440,6 +457,7 @@ struct ScfRun {
   double *S, *H, *X, *D, *F, *Fx, *P, *P2, *P3, *T1, *T2, *Dn, *Fbuf, *Ebuf;
   double *Bm, *coef, *enuc, *E, *dE, *dD, *err, *scale, *tr;
   int *nocc, *slot, *count;
+  int* active = nullptr;  // per molecule: 1 while iterating (null during set-up and the final gradient)
 
   dim3 elem_grid() const {
     const long long nn = (long long)nmax * nmax;
@@ -448,23 +466,23 @@ struct ScfRun {
   cudaError_t gemm(bool ta, bool tb, const double* A, const double* B, double* C, double alpha, double beta) const {
     const int t = (nmax + GT - 1) / GT;
     const dim3 grid(t, t, nmol);
-    if (!ta && !tb) gemm_packed_kernel<false, false><<<grid, 256, 0, st>>>(base, nm, A, B, C, alpha, beta);
-    else if (ta && !tb) gemm_packed_kernel<true, false><<<grid, 256, 0, st>>>(base, nm, A, B, C, alpha, beta);
-    else if (!ta && tb) gemm_packed_kernel<false, true><<<grid, 256, 0, st>>>(base, nm, A, B, C, alpha, beta);
-    else gemm_packed_kernel<true, true><<<grid, 256, 0, st>>>(base, nm, A, B, C, alpha, beta);
+    if (!ta && !tb) gemm_packed_kernel<false, false><<<grid, 256, 0, st>>>(base, nm, active, A, B, C, alpha, beta);
+    else if (ta && !tb) gemm_packed_kernel<true, false><<<grid, 256, 0, st>>>(base, nm, active, A, B, C, alpha, beta);
+    else if (!ta && tb) gemm_packed_kernel<false, true><<<grid, 256, 0, st>>>(base, nm, active, A, B, C, alpha, beta);
+    else gemm_packed_kernel<true, true><<<grid, 256, 0, st>>>(base, nm, active, A, B, C, alpha, beta);
     return cudaGetLastError();
   }
   // Dout = 2 X P X^T with P the purified projector of Fp (Fp is left intact);
   // iters purification steps (default purify_iters)
   cudaError_t purify_density(const double* Fp, double* Dout, int iters = 0) const {
     if (iters <= 0) iters = purify_iters;
-    purify_start_kernel<<<nmol, 256, 0, st>>>(base, nm, nocc, Fp, P);
+    purify_start_kernel<<<nmol, 256, 0, st>>>(base, nm, active, nocc, Fp, P);
     cudaError_t e = cudaGetLastError();
     for (int it = 0; it < iters && e == cudaSuccess; ++it) {
       if ((e = gemm(false, false, P, P, P2, 1.0, 0.0)) != cudaSuccess) break;
       if ((e = gemm(false, false, P2, P, P3, 1.0, 0.0)) != cudaSuccess) break;
-      purify_trace_kernel<<<nmol, 256, 0, st>>>(base, nm, P, P2, P3, tr);
-      purify_update_kernel<<<elem_grid(), 256, 0, st>>>(base, tr, P, P2, P3);
+      purify_trace_kernel<<<nmol, 256, 0, st>>>(base, nm, active, P, P2, P3, tr);
+      purify_update_kernel<<<elem_grid(), 256, 0, st>>>(base, active, tr, P, P2, P3);
       e = cudaGetLastError();
     }
     if (e != cudaSuccess) return e;
@@ -475,13 +493,13 @@ struct ScfRun {
   int step() {
     int rc = iqcp_fock_device(ctx, H, D, 1.0, F);
     if (rc) return rc;
-    energy_kernel<<<nmol, 256, 0, st>>>(base, D, H, F, enuc, E, dE);
+    energy_kernel<<<nmol, 256, 0, st>>>(base, active, D, H, F, enuc, E, dE);
     cudaError_t e = cudaGetLastError();
     // orthogonalised commutator X^T (F D S - S D F) X; (F D S)^T = S D F
     if (e == cudaSuccess) e = gemm(false, false, F, D, T1, 1.0, 0.0);
     if (e == cudaSuccess) e = gemm(false, false, T1, S, T2, 1.0, 0.0);
     if (e == cudaSuccess) {
-      antisym_kernel<<<elem_grid(), 256, 0, st>>>(base, nm, T2, T1);
+      antisym_kernel<<<elem_grid(), 256, 0, st>>>(base, nm, active, T2, T1);
       e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = gemm(true, false, X, T1, T2, 1.0, 0.0);
@@ -491,7 +509,7 @@ struct ScfRun {
       diis_store_kernel<<<2048, 256, 0, st>>>(total, slot, F, P2, Fbuf, Ebuf);
       diis_overlap_kernel<<<dim3(nmol, K), 256, 0, st>>>(base, total, K, slot, Ebuf, Bm);
       diis_solve_kernel<<<(nmol + 63) / 64, 64, 0, st>>>(nmol, K, count, Bm, coef);
-      diis_extrapolate_kernel<<<elem_grid(), 256, 0, st>>>(base, total, K, coef, Fbuf, Fx);
+      diis_extrapolate_kernel<<<elem_grid(), 256, 0, st>>>(base, active, total, K, coef, Fbuf, Fx);
       diis_advance_kernel<<<1, 1, 0, st>>>(K, slot, count);
       e = cudaGetLastError();
     }
@@ -500,7 +518,7 @@ struct ScfRun {
     if (e == cudaSuccess) e = gemm(false, false, T1, X, T2, 1.0, 0.0);
     if (e == cudaSuccess) e = purify_density(T2, Dn);
     if (e == cudaSuccess) {
-      rmsdiff_copy_kernel<<<nmol, 256, 0, st>>>(base, Dn, D, dD);
+      rmsdiff_copy_kernel<<<nmol, 256, 0, st>>>(base, active, Dn, D, dD);
       e = cudaGetLastError();
     }
     if (e != cudaSuccess) return ctx_fail(ctx, IQCP_ERR_CUDA, cudaGetErrorString(e));
@@ -577,6 +595,7 @@ int iqcp_batch_scf(iqcp_ctx* ctx, const iqcp_scf_options* opts_in, const double*
   int it = 0;
   bool all_conv = false;
   std::vector<char> conv(nmol, 0);
+  std::vector<int> h_active;
   r.ctx = ctx;
   r.nmol = nmol;
   r.K = opts.diis_size;
@@ -601,6 +620,8 @@ int iqcp_batch_scf(iqcp_ctx* ctx, const iqcp_scf_options* opts_in, const double*
   SCF_CK(buf.get(&r.nocc, nmol));
   SCF_CK(buf.get(&r.slot, 1));
   SCF_CK(buf.get(&r.count, 1));
+  int* d_active;
+  SCF_CK(buf.get(&d_active, nmol));
   SCF_CK(cudaMemsetAsync(r.Ebuf, 0, sizeof(double) * r.total * r.K, own));
   SCF_CK(cudaMemsetAsync(r.Fbuf, 0, sizeof(double) * r.total * r.K, own));
   SCF_CK(cudaMemsetAsync(r.Bm, 0, sizeof(double) * nmol * r.K * r.K, own));
@@ -658,7 +679,14 @@ int iqcp_batch_scf(iqcp_ctx* ctx, const iqcp_scf_options* opts_in, const double*
     // the core Hamiltonian's spectrum is wide next to its gap: more steps, once
     SCF_CK(r.purify_density(r.T2, r.D, 4 * opts.purify_iters));
   }
-  // iterations: the first eagerly (sets kernel attributes), then graph replays
+  // iterations: the first eagerly (sets kernel attributes), then graph replays.
+  // A geometry that meets the thresholds stops iterating, as rhf_scf stops per
+  // geometry: its flag turns 0 and every kernel of the iteration, the Fock
+  // build's quartet kernels included, skips it from the next replay on.
+  h_active.assign(nmol, 1);
+  SCF_CK(cudaMemcpyAsync(d_active, h_active.data(), sizeof(int) * nmol, cudaMemcpyHostToDevice, own));
+  r.active = d_active;
+  ctx_set_mol_active(ctx, d_active);
   for (it = 1; it <= opts.max_iter; ++it) {
     if (it == 1) {
       rc = r.step();
@@ -679,12 +707,22 @@ int iqcp_batch_scf(iqcp_ctx* ctx, const iqcp_scf_options* opts_in, const double*
     SCF_CK(cudaMemcpyAsync(host.data() + 2 * nmol, r.err, sizeof(double) * nmol, cudaMemcpyDeviceToHost, own));
     SCF_CK(cudaStreamSynchronize(own));
     all_conv = true;
+    bool frozen_now = false;
     for (int m = 0; m < nmol; ++m) {
+      if (!h_active[m]) continue;  // converged earlier
       conv[m] = std::fabs(host[m]) < opts.e_tol && host[nmol + m] < opts.d_tol && host[2 * nmol + m] < opts.err_tol;
       all_conv = all_conv && conv[m];
+      if (it > 2 && conv[m]) {
+        h_active[m] = 0;
+        frozen_now = true;
+      }
     }
     if (it > 2 && all_conv) break;
+    if (frozen_now)
+      SCF_CK(cudaMemcpyAsync(d_active, h_active.data(), sizeof(int) * nmol, cudaMemcpyHostToDevice, own));
   }
+  r.active = nullptr;
+  ctx_set_mol_active(ctx, nullptr);
   if (it > opts.max_iter) it = opts.max_iter;
   if (iterations) *iterations = it;
   if (energies) SCF_CK(cudaMemcpyAsync(energies, r.E, sizeof(double) * nmol, cudaMemcpyDeviceToHost, own));
@@ -709,6 +747,7 @@ int iqcp_batch_scf(iqcp_ctx* ctx, const iqcp_scf_options* opts_in, const double*
   if (converged)
     for (int m = 0; m < nmol; ++m) converged[m] = opts.max_iter > 0 ? conv[m] : 0;
 done:
+  ctx_set_mol_active(ctx, nullptr);
   if (exec) cudaGraphExecDestroy(exec);
   if (graph) cudaGraphDestroy(graph);
   if (own) cudaStreamSynchronize(own);
