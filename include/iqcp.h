@@ -224,7 +224,7 @@ int iqcp_eri_grad_device(iqcp_ctx* ctx, const double* d_D, double hf_frac, doubl
 /*
  * Batched RHF to self-consistency on the device: every geometry of the
  * context (batched or single) iterates together, one CUDA graph replay per
- * iteration (Fock build, energy, DIIS on X^T (FDS - SDF) X, density by
+ * iteration (Fock build, energy, DIIS on FDS - SDF, density by
  * canonical purification of X^T F X), with X = S^-1/2 from a Newton-Schulz
  * iteration and the core-Hamiltonian guess unless D0 is given.  Replaces the
  * per-geometry rhf_scf loop (scf/mod.rs:1363-1586) of the optimiser and scan

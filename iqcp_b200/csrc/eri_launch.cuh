@@ -102,7 +102,9 @@ cudaError_t launch_grad_variant(const GradArgs& args, cudaStream_t st) {
   // the team variant reads the Rys coefficients through L1 (no staged table)
   size_t fixed = sizeof(double) * rys_tab_doubles<NRG>();
   if (team) fixed = sizeof(double) * TG::WPB * TG::PER_WARP;
-  else if (wsh) fixed += sizeof(R) * grad_wsh_doubles<LA, LB, LC, LD>();
+  else if (wsh)
+    fixed = sizeof(double) * (grad_stages_rys<LA, LB, LC, LD, true>() ? rys_tab_doubles<NRG>() : 0) +
+            sizeof(R) * grad_wsh_doubles<LA, LB, LC, LD>();
   else if (group)
     fixed += sizeof(double) * (F32 ? GroupGrad<R, LA, LB, LC, LD, 8>::WDOUBLES : GroupGrad<R, LA, LB, LC, LD, 32>::WDOUBLES);
   // the per-block gradient accumulator only when it fits beside the tables

@@ -331,7 +331,13 @@ struct TeamGrad2 {
   static constexpr int QT = NT * RSZ * 4;                 // I, dA, dB, dC per unextended entry
   static constexpr int DBLK = C::NA * C::NB + C::NC * C::ND + C::NA * C::NC + C::NB * C::ND + C::NA * C::ND +
                               C::NB * C::NC;
-  static constexpr int PER_WARP = TAB + QT + ((DBLK + 3) / 4) * 4;
+  static constexpr int WOFF = TAB + QT + ((DBLK + 3) / 4) * 4;  // D x D weights of the quartet (NCOMP)
+  static constexpr int ROFF = WOFF + ((C::NCOMP + 1) / 2) * 2;  // Rys roots and weights of the primitive quartet
+  static constexpr int PER_WARP = ROFF + 2 * NR;
+  // phase B items: (root, bra component pair) looping over the ket components,
+  // or for kets of more than 9 components (root, bra pair, c) looping over d
+  static constexpr bool BYC = C::NC * C::ND > 9;
+  static constexpr int NITEM = NR * C::NA * C::NB * (BYC ? C::NC : 1);
   static constexpr int CPL = (C::NCOMP + 31) / 32;
   static constexpr int WPB = team_warps_per_block(PER_WARP);
   // resident blocks per SM asked of the compiler: what shared memory allows,
@@ -376,20 +382,8 @@ grad_team2_kernel(GradArgs args) {
   double* Dad = Dbd + C::NB * C::ND;
   double* Dbc = Dad + C::NA * C::ND;
 
-  // unextended table index of this lane's components, 7 bits per axis
-  int roffs[CPL];
-#pragma unroll
-  for (int m = 0; m < CPL; ++m) {
-    int comp = lane + 32 * m;
-    if (comp >= C::NCOMP) comp = 0;
-    const int d = comp % C::ND, c = (comp / C::ND) % C::NC, b = (comp / (C::ND * C::NC)) % C::NB,
-              a = comp / (C::ND * C::NC * C::NB);
-    int o = 0;
-#pragma unroll
-    for (int ax = 0; ax < 3; ++ax)
-      o |= TG::ridx(cart_pow(LA, a, ax), cart_pow(LB, b, ax), cart_pow(LC, c, ax), cart_pow(LD, d, ax)) << (7 * ax);
-    roffs[m] = o;
-  }
+  R* Wsh = reinterpret_cast<R*>(wbase + TG::WOFF);   // weights of the current quartet
+  double* rts = wbase + TG::ROFF;                    // t^2 and weight of each root
 
   for (int warp = next_task(args.next_task, lane); warp < args.ntasks; warp = next_task(args.next_task, lane)) {
   const QuartetTask task = args.tasks[warp];
@@ -424,33 +418,27 @@ grad_team2_kernel(GradArgs args) {
     for (int i = lane; i < C::NA * C::ND; i += 32) Dad[i] = __ldg(D + (bp.oa + i / C::ND) * n + kp.ob + i % C::ND);
     for (int i = lane; i < C::NB * C::NC; i += 32) Dbc[i] = __ldg(D + (bp.ob + i / C::NC) * n + kp.oa + i % C::NC);
     __syncwarp();
-    // D x D weights of this lane's components (compute_symmetry_weight, gradient.rs:1570-1640)
-    double W[CPL];
-#pragma unroll
-    for (int m = 0; m < CPL; ++m) {
-      const int comp = lane + 32 * m;
-      double t = 0.0;
-      if (comp < C::NCOMP) {
-        const int d = comp % C::ND, c = (comp / C::ND) % C::NC, b = (comp / (C::ND * C::NC)) % C::NB,
-                  a = comp / (C::ND * C::NC * C::NB);
-        const double dab = Dab[a * C::NB + b], dcd = Dcd[c * C::ND + d];
-        const double dac = Dac[a * C::NC + c], dbd = Dbd[b * C::ND + d];
-        const double dad = Dad[a * C::ND + d], dbc = Dbc[b * C::NC + c];
-        // w(p,q,r,s) = 1/2 D_pq D_rs - xs D_pr D_qs over the distinct permutations
-        t = 0.5 * dab * dcd - xs * dac * dbd;
-        if (!ij_same) t += 0.5 * dab * dcd - xs * dbc * dad;
-        if (!kl_same) t += 0.5 * dab * dcd - xs * dad * dbc;
-        if (!ij_same && !kl_same) t += 0.5 * dab * dcd - xs * dbd * dac;
-        if (!bk_same) {
-          t += 0.5 * dcd * dab - xs * dac * dbd;
-          if (!kl_same) t += 0.5 * dcd * dab - xs * dad * dbc;
-          if (!ij_same) t += 0.5 * dcd * dab - xs * dbc * dad;
-          if (!ij_same && !kl_same) t += 0.5 * dcd * dab - xs * dbd * dac;
-        }
-        const double angp = ang_factor(LA, a) * ang_factor(LB, b) * ang_factor(LC, c) * ang_factor(LD, d);
-        if (fabs(t / angp) < 1e-15) t = 0.0;  // |w| < 1e-15 skip on the reference weight
+    // D x D weights of the quartet's components into shared memory
+    // (compute_symmetry_weight, gradient.rs:1570-1640)
+    for (int comp = lane; comp < C::NCOMP; comp += 32) {
+      const int d = comp % C::ND, c = (comp / C::ND) % C::NC, b = (comp / (C::ND * C::NC)) % C::NB,
+                a = comp / (C::ND * C::NC * C::NB);
+      const double dab = Dab[a * C::NB + b], dcd = Dcd[c * C::ND + d];
+      const double dac = Dac[a * C::NC + c], dbd = Dbd[b * C::ND + d];
+      const double dad = Dad[a * C::ND + d], dbc = Dbc[b * C::NC + c];
+      // w(p,q,r,s) = 1/2 D_pq D_rs - xs D_pr D_qs over the distinct permutations
+      double t = 0.5 * dab * dcd - xs * dac * dbd;
+      if (!ij_same) t += 0.5 * dab * dcd - xs * dbc * dad;
+      if (!kl_same) t += 0.5 * dab * dcd - xs * dad * dbc;
+      if (!ij_same && !kl_same) t += 0.5 * dab * dcd - xs * dbd * dac;
+      if (!bk_same) {
+        t += 0.5 * dcd * dab - xs * dac * dbd;
+        if (!kl_same) t += 0.5 * dcd * dab - xs * dad * dbc;
+        if (!ij_same) t += 0.5 * dcd * dab - xs * dbc * dad;
+        if (!ij_same && !kl_same) t += 0.5 * dcd * dab - xs * dbd * dac;
       }
-      W[m] = t;
+      const double angp = ang_factor(LA, a) * ang_factor(LB, b) * ang_factor(LC, c) * ang_factor(LD, d);
+      Wsh[comp] = R(fabs(t / angp) < 1e-15 ? 0.0 : t);  // |w| < 1e-15 skip on the reference weight
     }
     double g[9];
 #pragma unroll
@@ -461,18 +449,23 @@ grad_team2_kernel(GradArgs args) {
       for (int j = 0; j < kp.np; ++j) {
         const PrimPair pk = load_pp(args.pp + kp.pstart + j);
         if (pb.K * pk.K < args.prim_thr) continue;
+        const double p = pb.p, q = pk.p, s = p + q;
+        const double PQ[3] = {pb.P[0] - pk.P[0], pb.P[1] - pk.P[1], pb.P[2] - pk.P[2]};
+        const double rs = rsqrt(s), inv_s = rs * rs;  // 1/(p+q), 1/sqrt(p+q): one rsqrt
+        __syncwarp();
+        if (lane < NR) {  // the Rys rule, one root per lane
+          const double T = p * q * inv_s * (PQ[0] * PQ[0] + PQ[1] * PQ[1] + PQ[2] * PQ[2]);
+          double t2, wr;
+          rys_rule_one_g<NR>(T, lane, &t2, &wr);
+          rts[2 * lane] = t2;
+          rts[2 * lane + 1] = wr;
+        }
         __syncwarp();
         // phase A: (root, axis, row a) slices of the extended tables, one per lane
         for (int task = lane; task < 3 * NR * (TG::EA + 1); task += 32) {
           const int a = task / (3 * NR), t = task - a * (3 * NR);
           const int r = t / 3, ax = t - 3 * r;
-          const double p = pb.p, q = pk.p, s = p + q;
-          const double PQ[3] = {pb.P[0] - pk.P[0], pb.P[1] - pk.P[1], pb.P[2] - pk.P[2]};
-          const double rs = rsqrt(s), inv_s = rs * rs;  // 1/(p+q), 1/sqrt(p+q): one rsqrt
-          const double rho = p * q * inv_s;
-          const double T = rho * (PQ[0] * PQ[0] + PQ[1] * PQ[1] + PQ[2] * PQ[2]);
-          double t2, wr;
-          rys_rule_one_g<NR>(T, r, &t2, &wr);
+          const double t2 = rts[2 * r], wr = rts[2 * r + 1];
           const double b00 = 0.5 * t2 * inv_s, h = 0.5 - 0.5 * t2;
           const double b10 = fma(h, pb.inv_p, b00), b01 = fma(h, pk.inv_p, b00);
           const double pa = pick3(ax, pb.P[0] - bp.A[0], pb.P[1] - bp.A[1], pb.P[2] - bp.A[2]);
@@ -515,28 +508,44 @@ grad_team2_kernel(GradArgs args) {
           }
         }
         __syncwarp();
+        // phase B: items (root, a, b[, c]); a lane loads each (I, dA, dB, dC) pair
+        // of its table rows once and reuses it over the ket components of the item
         R gl[9];
 #pragma unroll
         for (int x = 0; x < 9; ++x) gl[x] = R(0);
-#pragma unroll
-        for (int m = 0; m < CPL; ++m) {
-          if (W[m] == 0.0) continue;
-          const R w = R(W[m]);
-          const int o = roffs[m];
-#pragma unroll
-          for (int r = 0; r < NR; ++r) {
-            V2 v0[3], v1[3];
-#pragma unroll
-            for (int ax = 0; ax < 3; ++ax) {
-              const int t = r * 3 + ax, e = (o >> (7 * ax)) & 127;
-              v0[ax] = *reinterpret_cast<const V2*>(qt + ((2 * t) * RSZ + e) * 2);      // I, dI/dA
-              v1[ax] = *reinterpret_cast<const V2*>(qt + ((2 * t + 1) * RSZ + e) * 2);  // dI/dB, dI/dC
-            }
-            const R wyz = w * v0[1].x * v0[2].x, wxz = w * v0[0].x * v0[2].x, wxy = w * v0[0].x * v0[1].x;
-            gl[0] = fma(wyz, v0[0].y, gl[0]); gl[1] = fma(wxz, v0[1].y, gl[1]); gl[2] = fma(wxy, v0[2].y, gl[2]);
-            gl[3] = fma(wyz, v1[0].x, gl[3]); gl[4] = fma(wxz, v1[1].x, gl[4]); gl[5] = fma(wxy, v1[2].x, gl[5]);
-            gl[6] = fma(wyz, v1[0].y, gl[6]); gl[7] = fma(wxz, v1[1].y, gl[7]); gl[8] = fma(wxy, v1[2].y, gl[8]);
+        for (int item = lane; item < TG::NITEM; item += 32) {
+          int rest = item;
+          int c0 = 0;
+          if constexpr (TG::BYC) {
+            c0 = rest % C::NC;
+            rest /= C::NC;
           }
+          const int ab = rest % (C::NA * C::NB), r = rest / (C::NA * C::NB);
+          const int a = ab / C::NB, b = ab - a * C::NB;
+          int base[3];
+#pragma unroll
+          for (int ax = 0; ax < 3; ++ax)
+            base[ax] = TG::ridx(cart_pow(LA, a, ax), cart_pow(LB, b, ax), TG::BYC ? cart_pow(LC, c0, ax) : 0, 0);
+          const R* wrow = Wsh + ab * (C::NC * C::ND) + c0 * C::ND;
+#pragma unroll
+          for (int cc = 0; cc < (TG::BYC ? 1 : C::NC); ++cc)
+#pragma unroll
+            for (int d = 0; d < C::ND; ++d) {
+              const R w = wrow[cc * C::ND + d];
+              if (w == R(0)) continue;
+              V2 v0[3], v1[3];
+#pragma unroll
+              for (int ax = 0; ax < 3; ++ax) {
+                const int t = r * 3 + ax;
+                const int e = base[ax] + (TG::BYC ? 0 : cart_pow(LC, cc, ax)) * (LD + 1) + cart_pow(LD, d, ax);
+                v0[ax] = *reinterpret_cast<const V2*>(qt + ((2 * t) * RSZ + e) * 2);      // I, dI/dA
+                v1[ax] = *reinterpret_cast<const V2*>(qt + ((2 * t + 1) * RSZ + e) * 2);  // dI/dB, dI/dC
+              }
+              const R wyz = w * v0[1].x * v0[2].x, wxz = w * v0[0].x * v0[2].x, wxy = w * v0[0].x * v0[1].x;
+              gl[0] = fma(wyz, v0[0].y, gl[0]); gl[1] = fma(wxz, v0[1].y, gl[1]); gl[2] = fma(wxy, v0[2].y, gl[2]);
+              gl[3] = fma(wyz, v1[0].x, gl[3]); gl[4] = fma(wxz, v1[1].x, gl[4]); gl[5] = fma(wxy, v1[2].x, gl[5]);
+              gl[6] = fma(wyz, v1[0].y, gl[6]); gl[7] = fma(wxz, v1[1].y, gl[7]); gl[8] = fma(wxy, v1[2].y, gl[8]);
+            }
         }
 #pragma unroll
         for (int x = 0; x < 9; ++x) g[x] += double(gl[x]);

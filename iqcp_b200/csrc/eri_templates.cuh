@@ -486,6 +486,10 @@ template <int LA, int LB, int LC, int LD>
 __host__ __device__ constexpr int grad_wsh_doubles() {
   return 128 * ncart(LA) * ncart(LB) * ncart(LC) * ncart(LD);
 }
+template <int LA, int LB, int LC, int LD, bool WSH>
+__host__ __device__ constexpr bool grad_stages_rys() {
+  return !(WSH && ncart(LA) * ncart(LB) * ncart(LC) * ncart(LD) > 40);
+}
 
 template <typename R, int LA, int LB, int LC, int LD, int G, bool WSH = false>
 __global__ void __launch_bounds__(128, (LA + LB + LC + LD <= 1) ? 4 : 1) grad_kernel(GradArgs args) {
@@ -499,14 +503,18 @@ __global__ void __launch_bounds__(128, (LA + LB + LC + LD <= 1) ? 4 : 1) grad_ke
   constexpr int NG = 32 / G;
   constexpr bool F32 = sizeof(R) == 4;
   static_assert(!WSH || G == 1, "shared weights are per thread");
+  // large shared weight arrays leave no room for a second block beside the
+  // staged Rys table: those kernels read the table through L1 instead
+  constexpr bool STAGE = grad_stages_rys<LA, LB, LC, LD, WSH>();
   extern __shared__ double rtab[];
-  rys_stage_table<NR>(rtab);
+  if constexpr (STAGE) rys_stage_table<NR>(rtab);
+  constexpr int TABD = STAGE ? rys_tab_doubles<NR>() : 0;
   // weights of this thread's quartet: Wsh[c * 128] (WSH), as R
-  R* Wsh = reinterpret_cast<R*>(rtab + rys_tab_doubles<NR>()) + threadIdx.x;
+  R* Wsh = reinterpret_cast<R*>(rtab + TABD) + threadIdx.x;
   const volatile R* Wv = Wsh;
   // per-block gradient accumulator: many quartets hit the same few atoms, so
   // global atomics would serialise; one flush per block at the end instead
-  double* gacc = rtab + rys_tab_doubles<NR>() + (WSH ? grad_wsh_doubles<LA, LB, LC, LD>() * sizeof(R) / 8 : 0);
+  double* gacc = rtab + TABD + (WSH ? grad_wsh_doubles<LA, LB, LC, LD>() * sizeof(R) / 8 : 0);
   if (args.gsmem)
     for (int i = threadIdx.x; i < 3 * args.natoms; i += blockDim.x) gacc[i] = 0.0;
   __syncthreads();
@@ -596,7 +604,8 @@ __global__ void __launch_bounds__(128, (LA + LB + LC + LD <= 1) ? 4 : 1) grad_ke
         const double T = rho * (PQ[0] * PQ[0] + PQ[1] * PQ[1] + PQ[2] * PQ[2]);
         const double pref = kTwoPi52 * b.cK * k.cK * b.inv_p * k.inv_p * rs;
         double rt[NR], wt[NR];
-        rys_rule_tab<NR>(T, rtab, rt, wt);
+        if constexpr (STAGE) rys_rule_tab<NR>(T, rtab, rt, wt);
+        else rys_rule<NR>(T, rt, wt);
         const double PA[3] = {b.P[0] - bp.A[0], b.P[1] - bp.A[1], b.P[2] - bp.A[2]};
         const double QC[3] = {k.P[0] - kp.A[0], k.P[1] - kp.A[1], k.P[2] - kp.A[2]};
         const R a2 = R(2.0 * b.aa), b2 = R(2.0 * (b.p - b.aa)), c2 = R(2.0 * k.aa);

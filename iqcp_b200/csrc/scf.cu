@@ -8,9 +8,9 @@
 //
 //   1. F = H + J - K/2 of every geometry: iqcp_fock_device on the packed batch;
 //   2. E = 1/2 Tr D (H + F) + E_nuc (scf/mod.rs:898);
-//   3. Pulay DIIS (scf/mod.rs:1116-1327) on the orthogonalised commutator
-//      X^T (F D S - S D F) X, with a ring buffer of diis_size Fock matrices
-//      whose slot and fill count live on the device;
+//   3. Pulay DIIS (scf/mod.rs:1116-1327) on the AO commutator F D S - S D F
+//      (scf/mod.rs:990), with a ring buffer of diis_size Fock matrices whose
+//      slot and fill count live on the device;
 //   4. the new density without an eigensolver: canonical purification
 //      (Palser and Manolopoulos, Phys. Rev. B 58, 12704 (1998)) of
 //      F' = X^T F X, D = 2 X P X^T.  For a closed shell with a HOMO-LUMO gap, P
@@ -495,15 +495,13 @@ struct ScfRun {
     if (rc) return rc;
     energy_kernel<<<nmol, 256, 0, st>>>(base, active, D, H, F, enuc, E, dE);
     cudaError_t e = cudaGetLastError();
-    // orthogonalised commutator X^T (F D S - S D F) X; (F D S)^T = S D F
+    // DIIS error: the AO commutator F D S - S D F (scf/mod.rs:990); (F D S)^T = S D F
     if (e == cudaSuccess) e = gemm(false, false, F, D, T1, 1.0, 0.0);
     if (e == cudaSuccess) e = gemm(false, false, T1, S, T2, 1.0, 0.0);
     if (e == cudaSuccess) {
-      antisym_kernel<<<elem_grid(), 256, 0, st>>>(base, nm, active, T2, T1);
+      antisym_kernel<<<elem_grid(), 256, 0, st>>>(base, nm, active, T2, P2);
       e = cudaGetLastError();
     }
-    if (e == cudaSuccess) e = gemm(true, false, X, T1, T2, 1.0, 0.0);
-    if (e == cudaSuccess) e = gemm(false, false, T2, X, P2, 1.0, 0.0);
     if (e == cudaSuccess) {
       maxabs_kernel<<<nmol, 256, 0, st>>>(base, P2, err);
       diis_store_kernel<<<2048, 256, 0, st>>>(total, slot, F, P2, Fbuf, Ebuf);
