@@ -318,6 +318,10 @@ __host__ __device__ constexpr int team_warps_per_block(int per_warp) {
              : (team_resident(2, per_warp) >= team_resident(1, per_warp) && team_resident(2, per_warp) > 0 ? 2 : 1);
 }
 
+// Per-warp shared-memory budget (doubles) of the gradient team kernel; 20 KB
+// leaves room for about eleven resident warps per SM.
+constexpr int kTeamGradBudget = 2560;
+
 template <int LA, int LB, int LC, int LD>
 struct TeamGrad2 {
   using C = Cls<LA, LB, LC, LD>;
@@ -326,18 +330,36 @@ struct TeamGrad2 {
   static constexpr int TSZ = (EA + 1) * (EB + 1) * (EC + 1) * (ED + 1);
   static constexpr int SA = (EB + 1) * (EC + 1) * (ED + 1), SB = (EC + 1) * (ED + 1), SC = ED + 1;
   static constexpr int RSZ = (LA + 1) * (LB + 1) * (LC + 1) * (LD + 1);
-  static constexpr int NT = 3 * NR;                       // (root, axis) tables
-  static constexpr int TAB = ((NT * TSZ + 3) / 4) * 4;    // extended tables (doubles, padded)
-  static constexpr int QT = NT * RSZ * 4;                 // I, dA, dB, dC per unextended entry
+  // derivative tables: one row per bra index pair (ia, ib) of KQ = (LC+1)(LD+1)
+  // ket entries, rows KQP = KQ | 1 entries apart (an odd pitch spreads the rows
+  // that the lanes of a warp read over the shared-memory banks)
+  static constexpr int KQ = (LC + 1) * (LD + 1);
+  static constexpr int KQP = KQ | 1;
+  static constexpr int RSZP = (LA + 1) * (LB + 1) * KQP;
+  __host__ __device__ static constexpr int qpos(int e) { return (e / KQ) * KQP + e % KQ; }
   static constexpr int DBLK = C::NA * C::NB + C::NC * C::ND + C::NA * C::NC + C::NB * C::ND + C::NA * C::ND +
                               C::NB * C::NC;
+  // shared footprint (doubles) with the tables of rch roots at a time
+  static constexpr int footprint(int rch) {
+    return ((3 * rch * TSZ + 3) / 4) * 4 + 3 * rch * RSZP * 4 + ((DBLK + 3) / 4) * 4 + ((C::NCOMP + 1) / 2) * 2 +
+           2 * NR;
+  }
+  static constexpr int pick_rch(int rch) {
+    return (rch <= 1 || footprint(rch) <= kTeamGradBudget) ? rch : pick_rch(rch - 1);
+  }
+  // roots per pass of phases A, A2 and B: all of them, or as many as keep the
+  // per-warp tables within the budget (the (dd|..) and (dp|dp) classes)
+  static constexpr int RCH = pick_rch(NR);
+  static constexpr int NT = 3 * RCH;                      // (root, axis) tables of one pass
+  static constexpr int TAB = ((NT * TSZ + 3) / 4) * 4;    // extended tables (doubles, padded)
+  static constexpr int QT = NT * RSZP * 4;                // I, dA, dB, dC per unextended entry
   static constexpr int WOFF = TAB + QT + ((DBLK + 3) / 4) * 4;  // D x D weights of the quartet (NCOMP)
   static constexpr int ROFF = WOFF + ((C::NCOMP + 1) / 2) * 2;  // Rys roots and weights of the primitive quartet
   static constexpr int PER_WARP = ROFF + 2 * NR;
   // phase B items: (root, bra component pair) looping over the ket components,
   // or for kets of more than 9 components (root, bra pair, c) looping over d
   static constexpr bool BYC = C::NC * C::ND > 9;
-  static constexpr int NITEM = NR * C::NA * C::NB * (BYC ? C::NC : 1);
+  static constexpr int NITEM = RCH * C::NA * C::NB * (BYC ? C::NC : 1);  // per pass (whole chunk)
   static constexpr int CPL = (C::NCOMP + 31) / 32;
   static constexpr int WPB = team_warps_per_block(PER_WARP);
   // resident blocks per SM asked of the compiler: what shared memory allows,
@@ -460,11 +482,16 @@ grad_team2_kernel(GradArgs args) {
           rts[2 * lane] = t2;
           rts[2 * lane + 1] = wr;
         }
+        R gl[9];
+#pragma unroll
+        for (int x = 0; x < 9; ++x) gl[x] = R(0);
+        for (int r0 = 0; r0 < NR; r0 += TG::RCH) {  // roots in passes of RCH
+        const int nr = NR - r0 < TG::RCH ? NR - r0 : TG::RCH;
         __syncwarp();
         // phase A: (root, axis, row a) slices of the extended tables, one per lane
-        for (int task = lane; task < 3 * NR * (TG::EA + 1); task += 32) {
-          const int a = task / (3 * NR), t = task - a * (3 * NR);
-          const int r = t / 3, ax = t - 3 * r;
+        for (int task = lane; task < 3 * nr * (TG::EA + 1); task += 32) {
+          const int a = task / (3 * nr), t = task - a * (3 * nr);
+          const int r = r0 + t / 3, ax = t % 3;
           const double t2 = rts[2 * r], wr = rts[2 * r + 1];
           const double b00 = 0.5 * t2 * inv_s, h = 0.5 - 0.5 * t2;
           const double b10 = fma(h, pb.inv_p, b00), b01 = fma(h, pk.inv_p, b00);
@@ -490,7 +517,7 @@ grad_team2_kernel(GradArgs args) {
         // phase A2: I, dI/dA, dI/dB, dI/dC on the unextended indices
         {
           const R e2a = R(2.0 * pb.aa), e2b = R(2.0 * (pb.p - pb.aa)), e2c = R(2.0 * pk.aa);
-          for (int it = lane; it < 3 * NR * RSZ; it += 32) {
+          for (int it = lane; it < 3 * nr * RSZ; it += 32) {
             const int t = it / RSZ, e = it - t * RSZ;
             const int d = e % (LD + 1), c = (e / (LD + 1)) % (LC + 1), b = (e / ((LD + 1) * (LC + 1))) % (LB + 1),
                       a = e / ((LD + 1) * (LC + 1) * (LB + 1));
@@ -498,8 +525,8 @@ grad_team2_kernel(GradArgs args) {
             const int x = TG::eidx(a, b, c, d);
             // two planes of pairs per table, (I, dA) and (dB, dC), 2 * sizeof(R) apart
             // per entry, so that lanes reading different entries spread over the banks
-            R* q0 = qt + ((2 * t) * RSZ + e) * 2;
-            R* q1 = qt + ((2 * t + 1) * RSZ + e) * 2;
+            R* q0 = qt + ((2 * t) * TG::RSZP + TG::qpos(e)) * 2;
+            R* q1 = qt + ((2 * t + 1) * TG::RSZP + TG::qpos(e)) * 2;
             // power 0 has no lowered term; the index is clamped so no load leaves the table
             q0[0] = E[x];
             q0[1] = e2a * E[x + TG::SA] - R(a) * E[a ? x - TG::SA : x];
@@ -510,10 +537,8 @@ grad_team2_kernel(GradArgs args) {
         __syncwarp();
         // phase B: items (root, a, b[, c]); a lane loads each (I, dA, dB, dC) pair
         // of its table rows once and reuses it over the ket components of the item
-        R gl[9];
-#pragma unroll
-        for (int x = 0; x < 9; ++x) gl[x] = R(0);
-        for (int item = lane; item < TG::NITEM; item += 32) {
+        const int nitem = nr * (TG::NITEM / TG::RCH);
+        for (int item = lane; item < nitem; item += 32) {
           int rest = item;
           int c0 = 0;
           if constexpr (TG::BYC) {
@@ -522,24 +547,34 @@ grad_team2_kernel(GradArgs args) {
           }
           const int ab = rest % (C::NA * C::NB), r = rest / (C::NA * C::NB);
           const int a = ab / C::NB, b = ab - a * C::NB;
-          int base[3];
+          // this item's rows: QI (I, dA) and (dB, dC) pairs per axis, loaded once
+          constexpr int QI = TG::BYC ? LD + 1 : TG::KQ;
+          V2 q0[3][QI], q1[3][QI];
 #pragma unroll
-          for (int ax = 0; ax < 3; ++ax)
-            base[ax] = TG::ridx(cart_pow(LA, a, ax), cart_pow(LB, b, ax), TG::BYC ? cart_pow(LC, c0, ax) : 0, 0);
+          for (int ax = 0; ax < 3; ++ax) {
+            const int t = r * 3 + ax;
+            const int row = cart_pow(LA, a, ax) * (LB + 1) + cart_pow(LB, b, ax);
+            const int pos = row * TG::KQP + (TG::BYC ? cart_pow(LC, c0, ax) * (LD + 1) : 0);
+            const V2* p0 = reinterpret_cast<const V2*>(qt + ((2 * t) * TG::RSZP + pos) * 2);
+            const V2* p1 = reinterpret_cast<const V2*>(qt + ((2 * t + 1) * TG::RSZP + pos) * 2);
+#pragma unroll
+            for (int j = 0; j < QI; ++j) {
+              q0[ax][j] = p0[j];  // I, dI/dA
+              q1[ax][j] = p1[j];  // dI/dB, dI/dC
+            }
+          }
           const R* wrow = Wsh + ab * (C::NC * C::ND) + c0 * C::ND;
 #pragma unroll
           for (int cc = 0; cc < (TG::BYC ? 1 : C::NC); ++cc)
 #pragma unroll
             for (int d = 0; d < C::ND; ++d) {
               const R w = wrow[cc * C::ND + d];
-              if (w == R(0)) continue;
               V2 v0[3], v1[3];
 #pragma unroll
               for (int ax = 0; ax < 3; ++ax) {
-                const int t = r * 3 + ax;
-                const int e = base[ax] + (TG::BYC ? 0 : cart_pow(LC, cc, ax)) * (LD + 1) + cart_pow(LD, d, ax);
-                v0[ax] = *reinterpret_cast<const V2*>(qt + ((2 * t) * RSZ + e) * 2);      // I, dI/dA
-                v1[ax] = *reinterpret_cast<const V2*>(qt + ((2 * t + 1) * RSZ + e) * 2);  // dI/dB, dI/dC
+                const int j = (TG::BYC ? 0 : cart_pow(LC, cc, ax) * (LD + 1)) + cart_pow(LD, d, ax);
+                v0[ax] = q0[ax][j];
+                v1[ax] = q1[ax][j];
               }
               const R wyz = w * v0[1].x * v0[2].x, wxz = w * v0[0].x * v0[2].x, wxy = w * v0[0].x * v0[1].x;
               gl[0] = fma(wyz, v0[0].y, gl[0]); gl[1] = fma(wxz, v0[1].y, gl[1]); gl[2] = fma(wxy, v0[2].y, gl[2]);
@@ -547,6 +582,7 @@ grad_team2_kernel(GradArgs args) {
               gl[6] = fma(wyz, v1[0].y, gl[6]); gl[7] = fma(wxz, v1[1].y, gl[7]); gl[8] = fma(wxy, v1[2].y, gl[8]);
             }
         }
+        }  // root passes
 #pragma unroll
         for (int x = 0; x < 9; ++x) g[x] += double(gl[x]);
       }

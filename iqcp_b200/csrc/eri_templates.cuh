@@ -488,7 +488,7 @@ __host__ __device__ constexpr int grad_wsh_doubles() {
 }
 template <int LA, int LB, int LC, int LD, bool WSH>
 __host__ __device__ constexpr bool grad_stages_rys() {
-  return !(WSH && ncart(LA) * ncart(LB) * ncart(LC) * ncart(LD) > 40);
+  return !(WSH && ncart(LA) * ncart(LB) * ncart(LC) * ncart(LD) > 60);
 }
 
 template <typename R, int LA, int LB, int LC, int LD, int G, bool WSH = false>
@@ -503,8 +503,9 @@ __global__ void __launch_bounds__(128, (LA + LB + LC + LD <= 1) ? 4 : 1) grad_ke
   constexpr int NG = 32 / G;
   constexpr bool F32 = sizeof(R) == 4;
   static_assert(!WSH || G == 1, "shared weights are per thread");
-  // large shared weight arrays leave no room for a second block beside the
-  // staged Rys table: those kernels read the table through L1 instead
+  // large shared weight arrays (more than 60 components) leave no room for a
+  // second block beside the staged Rys table: those kernels read the table
+  // through L1 instead
   constexpr bool STAGE = grad_stages_rys<LA, LB, LC, LD, WSH>();
   extern __shared__ double rtab[];
   if constexpr (STAGE) rys_stage_table<NR>(rtab);
