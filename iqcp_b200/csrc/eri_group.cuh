@@ -56,7 +56,7 @@ template <typename R, int LA, int LB, int LC, int LD, int G>
 __global__ void __launch_bounds__(128) grad_group_kernel(GradArgs args) {
   using C = Cls<LA, LB, LC, LD>;
   using GG = GroupGrad<R, LA, LB, LC, LD, G>;
-  constexpr int EA = LA + 1, EB = LB + 1, EC = LC + 1, ED = LD;
+  constexpr int EA = LA + 1, EB = LB, EC = LC + 1, ED = LD;
   constexpr int ESZ = (EA + 1) * (EB + 1) * (EC + 1) * (ED + 1);
   constexpr int NR = GG::NR, NG = GG::NG;
   auto eidx = [](int a, int b, int c, int d) { return ((a * (EB + 1) + b) * (EC + 1) + c) * (ED + 1) + d; };
@@ -157,7 +157,7 @@ __global__ void __launch_bounds__(128) grad_group_kernel(GradArgs args) {
                   reg[ax] = E[ax][eidx(ia, ib, ic, id)];
                   dA[ax] = a2 * E[ax][eidx(ia + 1, ib, ic, id)] -
                            (ia > 0 ? R(ia) * E[ax][eidx(ia > 0 ? ia - 1 : 0, ib, ic, id)] : R(0));
-                  dB[ax] = b2 * E[ax][eidx(ia, ib + 1, ic, id)] -
+                  dB[ax] = b2 * (E[ax][eidx(ia + 1, ib, ic, id)] + R(AB[ax]) * E[ax][eidx(ia, ib, ic, id)]) -
                            (ib > 0 ? R(ib) * E[ax][eidx(ia, ib > 0 ? ib - 1 : 0, ic, id)] : R(0));
                   dC[ax] = c2 * E[ax][eidx(ia, ib, ic + 1, id)] -
                            (ic > 0 ? R(ic) * E[ax][eidx(ia, ib, ic > 0 ? ic - 1 : 0, id)] : R(0));

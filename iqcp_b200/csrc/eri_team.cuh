@@ -272,9 +272,10 @@ __global__ void __launch_bounds__(128) jk_team_kernel(JKArgs args) {
 // ---------------------------------------------------------------------------
 // Gradient team kernel with per-root derivative tables.
 //
-// Tables are extended by one on A, B and C (the D derivative follows from
-// translational invariance, dD = -(dA + dB + dC)), with one more root than the
-// energy (eri/mod.rs:2146-2149).  Per surviving primitive quartet:
+// Tables are extended by one on A and C (the B derivative takes I(a, b+1) =
+// I(a+1, b) + AB I(a, b) from the horizontal recurrence, the D derivative
+// follows from translational invariance, dD = -(dA + dB + dC)), with one more
+// root than the energy (eri/mod.rs:2146-2149).  Per surviving primitive quartet:
 //   phase A   the lanes build the extended 1D tables E of every (root, axis)
 //             in shared memory, one row a of a table per lane (axis_slice);
 //   phase A2  all 32 lanes turn them into, for every unextended index
@@ -325,7 +326,7 @@ constexpr int kTeamGradBudget = 2560;
 template <int LA, int LB, int LC, int LD>
 struct TeamGrad2 {
   using C = Cls<LA, LB, LC, LD>;
-  static constexpr int EA = LA + 1, EB = LB + 1, EC = LC + 1, ED = LD;
+  static constexpr int EA = LA + 1, EB = LB, EC = LC + 1, ED = LD;  // B derivative via I(a+1,b) + AB I(a,b)
   static constexpr int NR = (LA + LB + LC + LD + 2) / 2 + 1;
   static constexpr int TSZ = (EA + 1) * (EB + 1) * (EC + 1) * (ED + 1);
   static constexpr int SA = (EB + 1) * (EC + 1) * (ED + 1), SB = (EC + 1) * (ED + 1), SC = ED + 1;
@@ -519,6 +520,7 @@ grad_team2_kernel(GradArgs args) {
           const R e2a = R(2.0 * pb.aa), e2b = R(2.0 * (pb.p - pb.aa)), e2c = R(2.0 * pk.aa);
           for (int it = lane; it < 3 * nr * RSZ; it += 32) {
             const int t = it / RSZ, e = it - t * RSZ;
+            const R abx = R(pick3(t % 3, AB[0], AB[1], AB[2]));
             const int d = e % (LD + 1), c = (e / (LD + 1)) % (LC + 1), b = (e / ((LD + 1) * (LC + 1))) % (LB + 1),
                       a = e / ((LD + 1) * (LC + 1) * (LB + 1));
             const R* E = tab + t * TSZ;
@@ -530,7 +532,7 @@ grad_team2_kernel(GradArgs args) {
             // power 0 has no lowered term; the index is clamped so no load leaves the table
             q0[0] = E[x];
             q0[1] = e2a * E[x + TG::SA] - R(a) * E[a ? x - TG::SA : x];
-            q1[0] = e2b * E[x + TG::SB] - R(b) * E[b ? x - TG::SB : x];
+            q1[0] = e2b * (E[x + TG::SA] + abx * E[x]) - R(b) * E[b ? x - TG::SB : x];  // I(a, b+1) by the HRR
             q1[1] = e2c * E[x + TG::SC] - R(c) * E[c ? x - TG::SC : x];
           }
         }

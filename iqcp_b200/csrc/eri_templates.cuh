@@ -494,9 +494,10 @@ __host__ __device__ constexpr bool grad_stages_rys() {
 template <typename R, int LA, int LB, int LC, int LD, int G, bool WSH = false>
 __global__ void __launch_bounds__(128, (LA + LB + LC + LD <= 1) ? 4 : 1) grad_kernel(GradArgs args) {
   using C = Cls<LA, LB, LC, LD>;
-  // tables extended by one on A, B, C; the D derivative follows from
-  // translational invariance, so D needs no extension
-  constexpr int EA = LA + 1, EB = LB + 1, EC = LC + 1, ED = LD;
+  // tables extended by one on A and C; the B derivative takes I(a, b+1) from
+  // the horizontal recurrence, I(a+1, b) + AB I(a, b), and the D derivative
+  // follows from translational invariance
+  constexpr int EA = LA + 1, EB = LB, EC = LC + 1, ED = LD;
   constexpr int ESZ = (EA + 1) * (EB + 1) * (EC + 1) * (ED + 1);
   auto eidx = [](int a, int b, int c, int d) { return ((a * (EB + 1) + b) * (EC + 1) + c) * (ED + 1) + d; };
   constexpr int NR = (LA + LB + LC + LD + 2) / 2 + 1;
@@ -645,7 +646,7 @@ __global__ void __launch_bounds__(128, (LA + LB + LC + LD <= 1) ? 4 : 1) grad_ke
                     reg[ax] = E[ax][eidx(ia, ib, ic, id)];
                     dA[ax] = a2 * E[ax][eidx(ia + 1, ib, ic, id)] -
                              (ia > 0 ? R(ia) * E[ax][eidx(ia > 0 ? ia - 1 : 0, ib, ic, id)] : R(0));
-                    dB[ax] = b2 * E[ax][eidx(ia, ib + 1, ic, id)] -
+                    dB[ax] = b2 * (E[ax][eidx(ia + 1, ib, ic, id)] + R(AB[ax]) * E[ax][eidx(ia, ib, ic, id)]) -
                              (ib > 0 ? R(ib) * E[ax][eidx(ia, ib > 0 ? ib - 1 : 0, ic, id)] : R(0));
                     dC[ax] = c2 * E[ax][eidx(ia, ib, ic + 1, id)] -
                              (ic > 0 ? R(ic) * E[ax][eidx(ia, ib, ic > 0 ? ic - 1 : 0, id)] : R(0));
