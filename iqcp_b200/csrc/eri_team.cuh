@@ -47,7 +47,10 @@ __device__ __forceinline__ void rys_rule_one(double T, int r, const double* s, d
 template <int LA, int LB, int LC, int LD>
 struct TeamJK {
   using C = Cls<LA, LB, LC, LD>;
-  static constexpr int TAB = C::NR * 3 * C::TSZ;
+  // (root, axis) tables TSP = TSZ | 1 entries apart, so that the lanes of
+  // phase A, writing the same entry of consecutive tables, spread over the banks
+  static constexpr int TSP = C::TSZ | 1;
+  static constexpr int TAB = C::NR * 3 * TSP;
   static constexpr int BLK = C::NCOMP;
   static constexpr int WORK = TAB > BLK ? TAB : BLK;
   static constexpr int DB = C::NA * C::NB + C::NC * C::ND + C::NB * C::ND + C::NA * C::ND + C::NB * C::NC +
@@ -65,7 +68,7 @@ __device__ __forceinline__ void team_prim_loop(const JKArgs& args, const ShellPa
                                                const double* AB, const double* CD, const int* offs, double* acc,
                                                R* tab, int lane, const double* rtab) {
   using C = Cls<LA, LB, LC, LD>;
-  constexpr int NR = C::NR, TSZ = C::TSZ, CPL = TeamJK<LA, LB, LC, LD>::CPL;
+  constexpr int NR = C::NR, TSZ = TeamJK<LA, LB, LC, LD>::TSP, CPL = TeamJK<LA, LB, LC, LD>::CPL;
   for (int i = 0; i < bp.np; ++i) {
     const PrimPair pb = load_pp(args.pp + bp.pstart + i);
     for (int j = 0; j < kp.np; ++j) {
@@ -112,7 +115,7 @@ template <typename R, int LA, int LB, int LC, int LD, bool DO_K>
 __global__ void __launch_bounds__(128) jk_team_kernel(JKArgs args) {
   using C = Cls<LA, LB, LC, LD>;
   using TM = TeamJK<LA, LB, LC, LD>;
-  constexpr int NR = C::NR, TSZ = C::TSZ, CPL = TM::CPL;
+  constexpr int NR = C::NR, TSZ = TM::TSP, CPL = TM::CPL;  // table stride
   extern __shared__ double smem[];
   double* rtab = smem;
   rys_stage_table<NR>(rtab);
@@ -322,6 +325,9 @@ __host__ __device__ constexpr int team_warps_per_block(int per_warp) {
 // Per-warp shared-memory budget (doubles) of the gradient team kernel; 20 KB
 // leaves room for about eleven resident warps per SM.
 constexpr int kTeamGradBudget = 2560;
+// Largest extended table (entries) that one lane builds whole in registers
+// (the fused phase A): 72 doubles still compile without local memory.
+constexpr int kTeamFusedMaxTab = 72;
 
 template <int LA, int LB, int LC, int LD>
 struct TeamGrad2 {
@@ -329,6 +335,13 @@ struct TeamGrad2 {
   static constexpr int EA = LA + 1, EB = LB, EC = LC + 1, ED = LD;  // B derivative via I(a+1,b) + AB I(a,b)
   static constexpr int NR = (LA + LB + LC + LD + 2) / 2 + 1;
   static constexpr int TSZ = (EA + 1) * (EB + 1) * (EC + 1) * (ED + 1);
+  // extended tables TSP = TSZ | 1 entries apart: the lanes of phase A write the
+  // same entry of consecutive tables, which an even stride (48, 64, 72 ...)
+  // puts in one or two banks
+  static constexpr int TSP = TSZ | 1;
+  // fused phase A: one lane per (root, axis) builds its whole table in
+  // registers and writes the derivative planes itself (no shared E table)
+  static constexpr bool FUSED = TSZ <= kTeamFusedMaxTab;
   static constexpr int SA = (EB + 1) * (EC + 1) * (ED + 1), SB = (EC + 1) * (ED + 1), SC = ED + 1;
   static constexpr int RSZ = (LA + 1) * (LB + 1) * (LC + 1) * (LD + 1);
   // derivative tables: one row per bra index pair (ia, ib) of KQ = (LC+1)(LD+1)
@@ -342,7 +355,7 @@ struct TeamGrad2 {
                               C::NB * C::NC;
   // shared footprint (doubles) with the tables of rch roots at a time
   static constexpr int footprint(int rch) {
-    return ((3 * rch * TSZ + 3) / 4) * 4 + 3 * rch * RSZP * 4 + ((DBLK + 3) / 4) * 4 + ((C::NCOMP + 1) / 2) * 2 +
+    return (FUSED ? 0 : ((3 * rch * TSP + 3) / 4) * 4) + 3 * rch * RSZP * 4 + ((DBLK + 3) / 4) * 4 + ((C::NCOMP + 1) / 2) * 2 +
            2 * NR;
   }
   static constexpr int pick_rch(int rch) {
@@ -352,7 +365,7 @@ struct TeamGrad2 {
   // per-warp tables within the budget (the (dd|..) and (dp|dp) classes)
   static constexpr int RCH = pick_rch(NR);
   static constexpr int NT = 3 * RCH;                      // (root, axis) tables of one pass
-  static constexpr int TAB = ((NT * TSZ + 3) / 4) * 4;    // extended tables (doubles, padded)
+  static constexpr int TAB = FUSED ? 0 : ((NT * TSP + 3) / 4) * 4;  // extended tables (doubles, padded)
   static constexpr int QT = NT * RSZP * 4;                // I, dA, dB, dC per unextended entry
   static constexpr int WOFF = TAB + QT + ((DBLK + 3) / 4) * 4;  // D x D weights of the quartet (NCOMP)
   static constexpr int ROFF = WOFF + ((C::NCOMP + 1) / 2) * 2;  // Rys roots and weights of the primitive quartet
@@ -386,7 +399,7 @@ grad_team2_kernel(GradArgs args) {
   using C = Cls<LA, LB, LC, LD>;
   using TG = TeamGrad2<LA, LB, LC, LD>;
   using V2 = typename Vec2<R>::type;
-  constexpr int NR = TG::NR, TSZ = TG::TSZ, RSZ = TG::RSZ, CPL = TG::CPL;
+  constexpr int NR = TG::NR, RSZ = TG::RSZ, CPL = TG::CPL;
   extern __shared__ __align__(16) double smem[];
   const int wib = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
@@ -489,6 +502,43 @@ grad_team2_kernel(GradArgs args) {
         for (int r0 = 0; r0 < NR; r0 += TG::RCH) {  // roots in passes of RCH
         const int nr = NR - r0 < TG::RCH ? NR - r0 : TG::RCH;
         __syncwarp();
+        if constexpr (TG::FUSED) {
+          // phase A, fused: a lane per (root, axis) builds the whole extended
+          // table in registers and writes I, dI/dA, dI/dB, dI/dC of every
+          // unextended entry as two planes of pairs
+          const R e2a = R(2.0 * pb.aa), e2b = R(2.0 * (pb.p - pb.aa)), e2c = R(2.0 * pk.aa);
+          for (int t = lane; t < 3 * nr; t += 32) {
+            const int r = r0 + t / 3, ax = t % 3;
+            const double t2 = rts[2 * r], wr = rts[2 * r + 1];
+            const double b00 = 0.5 * t2 * inv_s, h = 0.5 - 0.5 * t2;
+            const double b10 = fma(h, pb.inv_p, b00), b01 = fma(h, pk.inv_p, b00);
+            const double pa = pick3(ax, pb.P[0] - bp.A[0], pb.P[1] - bp.A[1], pb.P[2] - bp.A[2]);
+            const double qc = pick3(ax, pk.P[0] - kp.A[0], pk.P[1] - kp.A[1], pk.P[2] - kp.A[2]);
+            const double pq = pick3(ax, PQ[0], PQ[1], PQ[2]);
+            const double g00 = ax == 2 ? wr * kTwoPi52 * pb.cK * pk.cK * pb.inv_p * pk.inv_p * rs : 1.0;
+            const R abx = R(pick3(ax, AB[0], AB[1], AB[2])), cdx = R(pick3(ax, CD[0], CD[1], CD[2]));
+            R E[TG::TSZ];
+            axis_table<R, TG::EA + TG::EB, TG::EC + TG::ED, TG::EA, TG::EB, TG::EC, TG::ED>(
+                R(pa - t2 * q * inv_s * pq), R(qc + t2 * p * inv_s * pq), R(b00), R(b10), R(b01), abx, cdx, R(g00),
+                E);
+            V2* q0 = reinterpret_cast<V2*>(qt + (2 * t) * TG::RSZP * 2);
+            V2* q1 = reinterpret_cast<V2*>(qt + (2 * t + 1) * TG::RSZP * 2);
+#pragma unroll
+            for (int e = 0; e < RSZ; ++e) {
+              const int d = e % (LD + 1), c = (e / (LD + 1)) % (LC + 1), b = (e / ((LD + 1) * (LC + 1))) % (LB + 1),
+                        a = e / ((LD + 1) * (LC + 1) * (LB + 1));
+              const int x = TG::eidx(a, b, c, d);
+              const R ex = E[x], ea = E[x + TG::SA];
+              V2 v0, v1;
+              v0.x = ex;
+              v0.y = a ? e2a * ea - R(a) * E[a ? x - TG::SA : x] : e2a * ea;
+              v1.x = b ? e2b * (ea + abx * ex) - R(b) * E[b ? x - TG::SB : x] : e2b * (ea + abx * ex);
+              v1.y = c ? e2c * E[x + TG::SC] - R(c) * E[c ? x - TG::SC : x] : e2c * E[x + TG::SC];
+              q0[TG::qpos(e)] = v0;
+              q1[TG::qpos(e)] = v1;
+            }
+          }
+        } else {
         // phase A: (root, axis, row a) slices of the extended tables, one per lane
         for (int task = lane; task < 3 * nr * (TG::EA + 1); task += 32) {
           const int a = task / (3 * nr), t = task - a * (3 * nr);
@@ -502,7 +552,7 @@ grad_team2_kernel(GradArgs args) {
           const double g00 = ax == 2 ? wr * kTwoPi52 * pb.cK * pk.cK * pb.inv_p * pk.inv_p * rs : 1.0;
           const R c00 = R(pa - t2 * q * inv_s * pq), c0p = R(qc + t2 * p * inv_s * pq);
           const R abx = R(pick3(ax, AB[0], AB[1], AB[2])), cdx = R(pick3(ax, CD[0], CD[1], CD[2]));
-          R* dst = tab + t * TSZ;
+          R* dst = tab + t * TG::TSP;
 #define IQCP_SLICE(AV)                                                                                  \
   axis_slice<R, LA + LB + 1, LC + LD + 1, TG::EA, TG::EB, TG::EC, TG::ED, AV>(                          \
       c00, c0p, R(b00), R(b10), R(b01), abx, cdx, R(g00), dst)
@@ -523,19 +573,24 @@ grad_team2_kernel(GradArgs args) {
             const R abx = R(pick3(t % 3, AB[0], AB[1], AB[2]));
             const int d = e % (LD + 1), c = (e / (LD + 1)) % (LC + 1), b = (e / ((LD + 1) * (LC + 1))) % (LB + 1),
                       a = e / ((LD + 1) * (LC + 1) * (LB + 1));
-            const R* E = tab + t * TSZ;
+            const R* E = tab + t * TG::TSP;
             const int x = TG::eidx(a, b, c, d);
             // two planes of pairs per table, (I, dA) and (dB, dC), 2 * sizeof(R) apart
             // per entry, so that lanes reading different entries spread over the banks
-            R* q0 = qt + ((2 * t) * TG::RSZP + TG::qpos(e)) * 2;
-            R* q1 = qt + ((2 * t + 1) * TG::RSZP + TG::qpos(e)) * 2;
+            V2* q0 = reinterpret_cast<V2*>(qt + ((2 * t) * TG::RSZP + TG::qpos(e)) * 2);
+            V2* q1 = reinterpret_cast<V2*>(qt + ((2 * t + 1) * TG::RSZP + TG::qpos(e)) * 2);
             // power 0 has no lowered term; the index is clamped so no load leaves the table
-            q0[0] = E[x];
-            q0[1] = e2a * E[x + TG::SA] - R(a) * E[a ? x - TG::SA : x];
-            q1[0] = e2b * (E[x + TG::SA] + abx * E[x]) - R(b) * E[b ? x - TG::SB : x];  // I(a, b+1) by the HRR
-            q1[1] = e2c * E[x + TG::SC] - R(c) * E[c ? x - TG::SC : x];
+            const R ex = E[x], ea = E[x + TG::SA];
+            V2 v0, v1;
+            v0.x = ex;
+            v0.y = e2a * ea - R(a) * E[a ? x - TG::SA : x];
+            v1.x = e2b * (ea + abx * ex) - R(b) * E[b ? x - TG::SB : x];  // I(a, b+1) by the HRR
+            v1.y = e2c * E[x + TG::SC] - R(c) * E[c ? x - TG::SC : x];
+            *q0 = v0;  // one paired store per plane
+            *q1 = v1;
           }
         }
+        }  // phase A
         __syncwarp();
         // phase B: items (root, a, b[, c]); a lane loads each (I, dA, dB, dC) pair
         // of its table rows once and reuses it over the ket components of the item

@@ -37,6 +37,8 @@ def lib():
             "or_max_threads": (ctypes.c_int, []),
             "or_boys_all": (None, [ctypes.c_int, ctypes.c_double, _dp_t]),
             "or_rys_roots": (ctypes.c_int, [ctypes.c_int, ctypes.c_double, _dp_t, _dp_t]),
+            "or_set_root_precision": (None, [ctypes.c_int]),
+            "or_root_precision": (ctypes.c_int, []),
             "or_cart_norm": (ctypes.c_double, [ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
             "or_shell_eri": (None, B + [ctypes.c_int] * 4 + [_dp_t, _llp_t]),
             "or_shell_eri_deriv": (None, B + [ctypes.c_int] * 4 + [_dp_t]),
@@ -74,6 +76,16 @@ def set_threads(n):
 
 def max_threads():
     return lib().or_max_threads()
+
+
+def set_root_precision(extended):
+    """Rys roots in the reference's double arithmetic (False, the default) or
+    the same algorithm in long double (True), for every later call."""
+    lib().or_set_root_precision(1 if extended else 0)
+
+
+def root_precision():
+    return bool(lib().or_root_precision())
 
 
 def boys_all(m_max, t):

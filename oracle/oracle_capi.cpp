@@ -47,6 +47,8 @@ int or_max_threads(void) {
 
 void or_boys_all(int m_max, double t, double* f) { boys_all(m_max, t, f); }
 
+void or_set_root_precision(int extended) { set_root_precision(extended); }
+int or_root_precision() { return root_precision(); }
 int or_rys_roots(int n, double t, double* roots, double* weights) {
   return rys_roots(n, t, roots, weights);
 }

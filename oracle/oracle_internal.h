@@ -21,6 +21,11 @@ constexpr int kMaxRoots = 10;       // rys/mod.rs:46 MAX_ROOTS
 void boys_all(int m_max, double t, double* f);                   // boys/mod.rs:587
 // Returns 0 on success, a negative code on RysError (rys/mod.rs:84-118).
 int rys_roots(int nroots, double t, double* roots, double* weights);  // rys/mod.rs:253
+// Working precision of rys_roots for the whole process: 0 = double, the
+// reference's arithmetic (default); 1 = the same algorithm in long double,
+// rounded to double at the end (a more accurate reading for diagnostics).
+void set_root_precision(int extended);
+int root_precision();
 
 // ---- basis ------------------------------------------------------------------
 struct Shell {

@@ -14,8 +14,16 @@ its Fock builder.
                  guess orbitals (float32; the density is 2 C C^T of their
                  float64 values) and the oracle's J and K there as row sums,
                  Tr(DJ), Tr(DK) and 20000 seeded element samples.
+  c5x            adds to config_c5.npz the same quantities with the oracle's
+                 Rys roots in extended precision (oracle.set_root_precision):
+                 the reference's double-precision moment method carries
+                 relative root errors up to ~2e-11 at five roots, which this
+                 workload's 3.6e9 shell quartets turn into J/K deviations of
+                 ~1e-9 on elements of order 10; the extended reading shows
+                 which side of a device/oracle difference that error is on.
 
-Usage: python tests/golden/make_config_fixtures.py [c2 c3 c5]   (about 2 h on 8 cores)
+Usage: python tests/golden/make_config_fixtures.py [c2 c3 c5 c5x]   (about 2 h on 8 cores,
+c5x about 1 h more)
 """
 import json
 import os
@@ -115,14 +123,41 @@ def c5_fixture(log):
                         tr_dk=float(np.sum(D * K)))
 
 
+def c5x_fixture(log):
+    path = os.path.join(HERE, "config_c5.npz")
+    f = dict(np.load(path))
+    meta = json.loads(str(f["meta"]))
+    atoms, basis = workload("c5", 0)
+    b = build_basis(atoms, basis)
+    C = f["c_occ_f32"].astype(np.float64)
+    D = 2.0 * C @ C.T
+    idx = f["idx"]
+    oracle.set_root_precision(True)
+    try:
+        t0 = time.time()
+        J, K, cnt = oracle.jk_direct(b, D)
+        t_jk = time.time() - t0
+    finally:
+        oracle.set_root_precision(False)
+    assert cnt[0] == 0
+    log("  oracle J/K, extended-precision roots: %.0f s" % t_jk)
+    meta["oracle_jk_extended_s"] = t_jk
+    meta["extended"] = "*_x: the same J/K with the Rys roots computed in long double"
+    f.update(meta=json.dumps(meta), j_sample_x=J[idx[:, 0], idx[:, 1]], k_sample_x=K[idx[:, 0], idx[:, 1]],
+             j_rowsum_x=J.sum(1), k_rowsum_x=K.sum(1), tr_dj_x=float(np.sum(D * J)), tr_dk_x=float(np.sum(D * K)))
+    np.savez_compressed(path, **f)
+
+
 def main():
-    which = sys.argv[1:] or ["c2", "c3", "c5"]
+    which = sys.argv[1:] or ["c2", "c3", "c5", "c5x"]
 
     def log(msg):
         print(msg, flush=True)
     for name in which:
         if name == "c5":
             c5_fixture(log)
+        elif name == "c5x":
+            c5x_fixture(log)
         else:
             scf_fixture(name, log)
 
