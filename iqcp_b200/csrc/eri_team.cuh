@@ -326,8 +326,9 @@ __host__ __device__ constexpr int team_warps_per_block(int per_warp) {
 // leaves room for about eleven resident warps per SM.
 constexpr int kTeamGradBudget = 2560;
 // Largest extended table (entries) that one lane builds whole in registers
-// (the fused phase A): 72 doubles still compile without local memory.
-constexpr int kTeamFusedMaxTab = 72;
+// (the fused phase A); up to 96 the spill is a few hundred bytes, which costs
+// less than the shared table it replaces.
+constexpr int kTeamFusedMaxTab = 96;
 
 template <int LA, int LB, int LC, int LD>
 struct TeamGrad2 {
@@ -351,11 +352,16 @@ struct TeamGrad2 {
   static constexpr int KQP = KQ | 1;
   static constexpr int RSZP = (LA + 1) * (LB + 1) * KQP;
   __host__ __device__ static constexpr int qpos(int e) { return (e / KQ) * KQP + e % KQ; }
+  // pair (I, dA) / (dB, dC) index of entry position pos in plane pl of table t:
+  // planes RSZP + 1 pairs apart and tables 2 RSZP + 1, so the lanes of the
+  // fused phase A (one table each) store to different banks
+  static constexpr int PSTR = RSZP + 1, TSTR = 2 * RSZP + 1;
+  __host__ __device__ static constexpr int pair(int t, int pl, int pos) { return t * TSTR + pl * PSTR + pos; }
   static constexpr int DBLK = C::NA * C::NB + C::NC * C::ND + C::NA * C::NC + C::NB * C::ND + C::NA * C::ND +
                               C::NB * C::NC;
   // shared footprint (doubles) with the tables of rch roots at a time
   static constexpr int footprint(int rch) {
-    return (FUSED ? 0 : ((3 * rch * TSP + 3) / 4) * 4) + 3 * rch * RSZP * 4 + ((DBLK + 3) / 4) * 4 + ((C::NCOMP + 1) / 2) * 2 +
+    return (FUSED ? 0 : ((3 * rch * TSP + 3) / 4) * 4) + ((3 * rch * TSTR * 2 + 3) / 4) * 4 + ((DBLK + 3) / 4) * 4 + ((C::NCOMP + 1) / 2) * 2 +
            2 * NR;
   }
   static constexpr int pick_rch(int rch) {
@@ -366,7 +372,7 @@ struct TeamGrad2 {
   static constexpr int RCH = pick_rch(NR);
   static constexpr int NT = 3 * RCH;                      // (root, axis) tables of one pass
   static constexpr int TAB = FUSED ? 0 : ((NT * TSP + 3) / 4) * 4;  // extended tables (doubles, padded)
-  static constexpr int QT = NT * RSZP * 4;                // I, dA, dB, dC per unextended entry
+  static constexpr int QT = ((NT * TSTR * 2 + 3) / 4) * 4;  // I, dA, dB, dC per unextended entry
   static constexpr int WOFF = TAB + QT + ((DBLK + 3) / 4) * 4;  // D x D weights of the quartet (NCOMP)
   static constexpr int ROFF = WOFF + ((C::NCOMP + 1) / 2) * 2;  // Rys roots and weights of the primitive quartet
   static constexpr int PER_WARP = ROFF + 2 * NR;
@@ -521,8 +527,8 @@ grad_team2_kernel(GradArgs args) {
             axis_table<R, TG::EA + TG::EB, TG::EC + TG::ED, TG::EA, TG::EB, TG::EC, TG::ED>(
                 R(pa - t2 * q * inv_s * pq), R(qc + t2 * p * inv_s * pq), R(b00), R(b10), R(b01), abx, cdx, R(g00),
                 E);
-            V2* q0 = reinterpret_cast<V2*>(qt + (2 * t) * TG::RSZP * 2);
-            V2* q1 = reinterpret_cast<V2*>(qt + (2 * t + 1) * TG::RSZP * 2);
+            V2* q0 = reinterpret_cast<V2*>(qt + TG::pair(t, 0, 0) * 2);
+            V2* q1 = reinterpret_cast<V2*>(qt + TG::pair(t, 1, 0) * 2);
 #pragma unroll
             for (int e = 0; e < RSZ; ++e) {
               const int d = e % (LD + 1), c = (e / (LD + 1)) % (LC + 1), b = (e / ((LD + 1) * (LC + 1))) % (LB + 1),
@@ -577,8 +583,8 @@ grad_team2_kernel(GradArgs args) {
             const int x = TG::eidx(a, b, c, d);
             // two planes of pairs per table, (I, dA) and (dB, dC), 2 * sizeof(R) apart
             // per entry, so that lanes reading different entries spread over the banks
-            V2* q0 = reinterpret_cast<V2*>(qt + ((2 * t) * TG::RSZP + TG::qpos(e)) * 2);
-            V2* q1 = reinterpret_cast<V2*>(qt + ((2 * t + 1) * TG::RSZP + TG::qpos(e)) * 2);
+            V2* q0 = reinterpret_cast<V2*>(qt + TG::pair(t, 0, TG::qpos(e)) * 2);
+            V2* q1 = reinterpret_cast<V2*>(qt + TG::pair(t, 1, TG::qpos(e)) * 2);
             // power 0 has no lowered term; the index is clamped so no load leaves the table
             const R ex = E[x], ea = E[x + TG::SA];
             V2 v0, v1;
@@ -612,8 +618,8 @@ grad_team2_kernel(GradArgs args) {
             const int t = r * 3 + ax;
             const int row = cart_pow(LA, a, ax) * (LB + 1) + cart_pow(LB, b, ax);
             const int pos = row * TG::KQP + (TG::BYC ? cart_pow(LC, c0, ax) * (LD + 1) : 0);
-            const V2* p0 = reinterpret_cast<const V2*>(qt + ((2 * t) * TG::RSZP + pos) * 2);
-            const V2* p1 = reinterpret_cast<const V2*>(qt + ((2 * t + 1) * TG::RSZP + pos) * 2);
+            const V2* p0 = reinterpret_cast<const V2*>(qt + TG::pair(t, 0, pos) * 2);
+            const V2* p1 = reinterpret_cast<const V2*>(qt + TG::pair(t, 1, pos) * 2);
 #pragma unroll
             for (int j = 0; j < QI; ++j) {
               q0[ax][j] = p0[j];  // I, dI/dA
