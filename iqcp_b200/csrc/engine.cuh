@@ -21,6 +21,13 @@ constexpr int kNumPairClasses = 6;
 constexpr int kMaxL = 2;
 
 __host__ __device__ constexpr int ncart(int l) { return (l + 1) * (l + 2) / 2; }
+// Rys roots of the first-derivative integrals.  Every product the gradient
+// contracts has one index raised by one, total angular momentum L + 1, i.e. a
+// polynomial of degree L + 1 in t^2, which an n-point rule integrates exactly
+// once 2n - 1 >= L + 1.  (The reference takes L/2 + 2 for even L,
+// integrals/eri/mod.rs:2146-2147, one root more than exactness needs; the
+// results agree to rounding.)
+__host__ __device__ constexpr int grad_nroots(int L) { return (L + 1) / 2 + 1; }
 __host__ __device__ constexpr int pair_class(int la, int lb) { return la * (la + 1) / 2 + lb; }
 __host__ __device__ constexpr int class_la(int c) { return c == 0 ? 0 : (c <= 2 ? 1 : 2); }
 __host__ __device__ constexpr int class_lb(int c) { return c - class_la(c) * (class_la(c) + 1) / 2; }

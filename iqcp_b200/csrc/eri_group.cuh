@@ -20,7 +20,7 @@ template <typename R, int LA, int LB, int LC, int LD, int G>
 struct GroupGrad {
   using C = Cls<LA, LB, LC, LD>;
   static constexpr int NG = 32 / G;                                   // groups per warp
-  static constexpr int NR = (LA + LB + LC + LD + 2) / 2 + 1;
+  static constexpr int NR = grad_nroots(LA + LB + LC + LD);
   static constexpr int WDOUBLES = (4 * NG * C::NCOMP * (int)sizeof(R) + 15) / 16 * 2;  // 4 warps per block
 };
 

@@ -93,7 +93,7 @@ template <typename R, int LA, int LB, int LC, int LD>
 cudaError_t launch_grad_variant(const GradArgs& args, cudaStream_t st) {
   using C = Cls<LA, LB, LC, LD>;
   constexpr bool F32 = sizeof(R) == 4;
-  constexpr int NRG = (LA + LB + LC + LD + 2) / 2 + 1;
+  constexpr int NRG = grad_nroots(LA + LB + LC + LD);
   constexpr bool WSH_OK = !F32 && C::NCOMP >= kWshMinComp && C::NCOMP <= kWshMaxComp;
   using TG = TeamGrad2<LA, LB, LC, LD>;
   const bool team = args.mode == 1 || (F32 && C::NCOMP > 324);

@@ -277,10 +277,14 @@ __global__ void __launch_bounds__(128) jk_team_kernel(JKArgs args) {
 //
 // Tables are extended by one on A and C (the B derivative takes I(a, b+1) =
 // I(a+1, b) + AB I(a, b) from the horizontal recurrence, the D derivative
-// follows from translational invariance, dD = -(dA + dB + dC)), with one more
-// root than the energy (eri/mod.rs:2146-2149).  Per surviving primitive quartet:
-//   phase A   the lanes build the extended 1D tables E of every (root, axis)
-//             in shared memory, one row a of a table per lane (axis_slice);
+// follows from translational invariance, dD = -(dA + dB + dC)), with the
+// roots of total angular momentum L + 1 (grad_nroots).  Per surviving
+// primitive quartet:
+//   phase A   fused (tables of <= kTeamFusedMaxTab entries): a lane per
+//             (root, axis) builds the whole extended table in registers and
+//             writes the four derivative planes below itself; otherwise the
+//             lanes build the tables E in shared memory, one row a of a table
+//             per lane (axis_slice), and
 //   phase A2  all 32 lanes turn them into, for every unextended index
 //             (ia, ib, ic, id), the four values I, dI/dA, dI/dB, dI/dC
 //             (d/dA: 2a E(ia+1) - ia E(ia-1), likewise B, C), stored as two
@@ -334,7 +338,7 @@ template <int LA, int LB, int LC, int LD>
 struct TeamGrad2 {
   using C = Cls<LA, LB, LC, LD>;
   static constexpr int EA = LA + 1, EB = LB, EC = LC + 1, ED = LD;  // B derivative via I(a+1,b) + AB I(a,b)
-  static constexpr int NR = (LA + LB + LC + LD + 2) / 2 + 1;
+  static constexpr int NR = grad_nroots(LA + LB + LC + LD);
   static constexpr int TSZ = (EA + 1) * (EB + 1) * (EC + 1) * (ED + 1);
   // extended tables TSP = TSZ | 1 entries apart: the lanes of phase A write the
   // same entry of consecutive tables, which an even stride (48, 64, 72 ...)

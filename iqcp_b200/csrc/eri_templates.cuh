@@ -500,7 +500,7 @@ __global__ void __launch_bounds__(128, (LA + LB + LC + LD <= 1) ? 4 : 1) grad_ke
   constexpr int EA = LA + 1, EB = LB, EC = LC + 1, ED = LD;
   constexpr int ESZ = (EA + 1) * (EB + 1) * (EC + 1) * (ED + 1);
   auto eidx = [](int a, int b, int c, int d) { return ((a * (EB + 1) + b) * (EC + 1) + c) * (ED + 1) + d; };
-  constexpr int NR = (LA + LB + LC + LD + 2) / 2 + 1;
+  constexpr int NR = grad_nroots(LA + LB + LC + LD);
   constexpr int NG = 32 / G;
   constexpr bool F32 = sizeof(R) == 4;
   static_assert(!WSH || G == 1, "shared weights are per thread");

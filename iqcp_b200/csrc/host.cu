@@ -1445,7 +1445,7 @@ static int count_prim_quartets(iqcp_ctx* ctx) {
 //   VRR(nb,nk) = 4 max(nb-1,0) + [nk>0](1 + 4(nk-1)) + 7 nb nk
 //   HTR1(j,l)  = (j+1) l (l+1) + j (j+1)
 // plus 12 per contracted integral for the 8-fold J/K digestion.  Gradient:
-// tables extended by one on bra and ket, one more root, and per component
+// tables extended by one on bra and ket, the reference's root count, and per component
 // 4 centres x 3 axes of (2 HTR1 + 7), digested with 12 FMAs per component.
 static double vrr_cost(int nb, int nk) {
   return 4.0 * (nb > 1 ? nb - 1 : 0) + (nk > 0 ? 1.0 + 4.0 * (nk - 1) : 0.0) + 7.0 * nb * nk;
@@ -1455,6 +1455,8 @@ static double htr1(int j, int l) { return double((j + 1) * l * (l + 1) + j * (j 
 static void class_cost(int X, int Y, bool grad, double* per_prim, double* per_quartet) {
   const int la = class_la(X), lb = class_lb(X), lc = class_la(Y), ld = class_lb(Y);
   const int L = la + lb + lc + ld;
+  // the reference's root counts (eri/mod.rs:2146-2147 for the gradient): the
+  // model counts the reference's work, whatever the kernels save
   const int nr = grad ? (L + 2) / 2 + 1 : L / 2 + 1;
   const int nb = la + lb + (grad ? 1 : 0), nk = lc + ld + (grad ? 1 : 0);
   double comp = 0.0;
