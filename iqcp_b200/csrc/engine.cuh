@@ -142,6 +142,7 @@ struct JKArgs {
   int mode;          // kernel variant: 0 thread per quartet, 1 warp-cooperative, 2/3: 8/32 lanes per quartet
   Mixed mx;
   int* next_task;             // work counter (zeroed before the launch)
+  int ket_split = 1;          // team kernels: warps per task, each taking a slice of its kets
   const long long* mol_base;  // per molecule: offset of its nbf x nbf block in D, J, K
   const int* mol_n;           // per molecule: nbf (row stride of its block)
   int nset;                   // densities digested per quartet (1, or several response densities)
@@ -181,6 +182,7 @@ struct GradArgs {
   int gsmem;
   Mixed mx;
   int* next_task;    // work counter (zeroed before the launch)
+  int ket_split = 1;  // team kernel: warps per task, each taking a slice of its kets
   const long long* mol_base;  // per molecule: offset of its block in D
   const int* mol_n;           // per molecule: nbf
 };

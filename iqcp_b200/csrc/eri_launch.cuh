@@ -36,6 +36,32 @@ inline int persistent_blocks(K kernel, size_t smem, int ntasks, int threads = 12
   } while (0)
 #define IQCP_LAUNCH(KERNEL, SMEM, ARGS, ST) IQCP_LAUNCH_T(KERNEL, 128, SMEM, ARGS, ST)
 
+// Team kernels walk a task's kets in one warp, one after the other.  A class
+// with fewer tasks than twice the resident warps ((dd|dd) on a 40-atom
+// molecule: ~700 tasks for ~1300 warps) would leave SMs idle and end on its
+// longest task, so its tasks are split into 2, 4 or 8 slices of kets, each
+// a work item of its own.
+template <typename K>
+inline int team_ket_split(K kernel, size_t smem, int ntasks, int threads) {
+  int per_sm = 0, dev = 0, sms = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const long long warps = (long long)(per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1) * (threads / 32);
+  int s = 1;
+  while (s < 8 && (long long)ntasks * s < 2 * warps) s *= 2;
+  return s;
+}
+
+#define IQCP_LAUNCH_TEAM(KERNEL, THREADS, SMEM, ARGS, ST)                                                \
+  do {                                                                                                   \
+    cudaError_t e_ = set_smem(KERNEL, SMEM);                                                             \
+    if (e_ != cudaSuccess) return e_;                                                                    \
+    (ARGS).ket_split = team_ket_split(KERNEL, SMEM, (ARGS).ntasks, THREADS);                             \
+    KERNEL<<<persistent_blocks(KERNEL, SMEM, (ARGS).ntasks * (ARGS).ket_split, THREADS), THREADS, SMEM, \
+             ST>>>(ARGS);                                                                                \
+  } while (0)
+
 // mode: 0 one quartet per thread, 1 warp-cooperative (eri_team.cuh),
 // 2 / 3 eight / thirty-two lanes share one quartet's primitive quartets
 // (J/K: small classes only; gradient: see launch_grad_variant; requests a
@@ -50,8 +76,9 @@ cudaError_t launch_jk_variant(const JKArgs& a, cudaStream_t st) {
   const bool team = a.mode == 1 || (F32 && C::NCOMP > 324);
   if (team) {
     const size_t bytes = sizeof(double) * 4 * TeamJK<LA, LB, LC, LD>::PER_WARP + tb;
-    if (a.K) IQCP_LAUNCH((jk_team_kernel<R, LA, LB, LC, LD, true>), bytes, a, st);
-    else IQCP_LAUNCH((jk_team_kernel<R, LA, LB, LC, LD, false>), bytes, a, st);
+    JKArgs b = a;
+    if (a.K) IQCP_LAUNCH_TEAM((jk_team_kernel<R, LA, LB, LC, LD, true>), 128, bytes, b, st);
+    else IQCP_LAUNCH_TEAM((jk_team_kernel<R, LA, LB, LC, LD, false>), 128, bytes, b, st);
   } else if (C::NCOMP <= 27 && (a.mode == 2 || a.mode == 3)) {
     if constexpr (C::NCOMP <= 27) {
       if (a.mode == 2 || F32) {
@@ -113,7 +140,7 @@ cudaError_t launch_grad_variant(const GradArgs& args, cudaStream_t st) {
   const size_t gacc = a.gsmem ? sizeof(double) * 3 * a.natoms : 0;
   const size_t bytes = fixed + gacc;
   if (team) {
-    IQCP_LAUNCH_T((grad_team2_kernel<R, LA, LB, LC, LD>), 32 * TG::WPB, bytes, a, st);
+    IQCP_LAUNCH_TEAM((grad_team2_kernel<R, LA, LB, LC, LD>), 32 * TG::WPB, bytes, a, st);
   } else if (wsh) {
     if constexpr (WSH_OK) IQCP_LAUNCH((grad_kernel<R, LA, LB, LC, LD, 1, true>), bytes, a, st);
   } else if (group) {

@@ -146,10 +146,14 @@ __global__ void __launch_bounds__(128) jk_team_kernel(JKArgs args) {
     offs[m] = o;
   }
 
-  for (int warp = next_task(args.next_task, lane); warp < args.ntasks; warp = next_task(args.next_task, lane)) {
+  const int S = args.ket_split;  // work items per task (slices of its kets)
+  for (int item = next_task(args.next_task, lane); item < args.ntasks * S; item = next_task(args.next_task, lane)) {
+  const int warp = item / S;     // the task
   const QuartetTask task = args.tasks[warp];
   const ShellPair bp = args.pairs[task.bra];
   if (task_inactive(args.mol_active, bp.mol)) continue;
+  const int kper = (task.nket + S - 1) / S, k_lo = (item - warp * S) * kper;
+  const int k_hi = task.nket < k_lo + kper ? task.nket : k_lo + kper;
   // this task's molecule block (bra and ket pairs always share a molecule)
   const int n = args.mol_n[bp.mol];
   const long long mb = args.mol_base[bp.mol];
@@ -161,7 +165,7 @@ __global__ void __launch_bounds__(128) jk_team_kernel(JKArgs args) {
 
   int nf32 = 0;
   const unsigned sel = task_sel(args.mx, warp, task.nket);
-  for (int kk = 0; kk < task.nket; ++kk) {
+  for (int kk = k_lo; kk < k_hi; ++kk) {
     if (!((sel >> kk) & 1u)) continue;  // another pass's ket (the same on every lane)
     const int kpos = task.ket0 + kk;
     const ShellPair kp = args.pairs[__ldg(args.ket_list + kpos)];
@@ -438,9 +442,13 @@ grad_team2_kernel(GradArgs args) {
   R* Wsh = reinterpret_cast<R*>(wbase + TG::WOFF);   // weights of the current quartet
   double* rts_all = wbase + TG::ROFF;                // t^2 and weight of each (ket primitive, root)
 
-  for (int warp = next_task(args.next_task, lane); warp < args.ntasks; warp = next_task(args.next_task, lane)) {
+  const int S = args.ket_split;  // work items per task (slices of its kets)
+  for (int item = next_task(args.next_task, lane); item < args.ntasks * S; item = next_task(args.next_task, lane)) {
+  const int warp = item / S;     // the task
   const QuartetTask task = args.tasks[warp];
   const ShellPair bp = args.pairs[task.bra];
+  const int kper = (task.nket + S - 1) / S, k_lo = (item - warp * S) * kper;
+  const int k_hi = task.nket < k_lo + kper ? task.nket : k_lo + kper;
   // this task's molecule block (bra and ket pairs always share a molecule)
   const int n = args.mol_n[bp.mol];
   const long long mb = args.mol_base[bp.mol];
@@ -454,7 +462,7 @@ grad_team2_kernel(GradArgs args) {
   int nsel = 0;
   const unsigned sel = task_sel(args.mx, warp, task.nket);
 
-  for (int kk = 0; kk < task.nket; ++kk) {
+  for (int kk = k_lo; kk < k_hi; ++kk) {
     if (!((sel >> kk) & 1u)) continue;  // another pass's ket (the same on every lane)
     const int kpos = task.ket0 + kk;
     const ShellPair kp = args.pairs[__ldg(args.ket_list + kpos)];

@@ -491,6 +491,9 @@ __host__ __device__ constexpr bool grad_stages_rys() {
   return !(WSH && ncart(LA) * ncart(LB) * ncart(LC) * ncart(LD) > 60);
 }
 
+// Resident blocks asked of the compiler: 4 for L <= 1 (for (ps|ss) the
+// 128-register cap spills 76 bytes per thread, and is still faster than 3
+// blocks without spill: 4.2 against 4.4 ms on the 40-atom step); 1 above.
 template <typename R, int LA, int LB, int LC, int LD, int G, bool WSH = false>
 __global__ void __launch_bounds__(128, (LA + LB + LC + LD <= 1) ? 4 : 1) grad_kernel(GradArgs args) {
   using C = Cls<LA, LB, LC, LD>;

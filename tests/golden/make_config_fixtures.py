@@ -10,17 +10,14 @@ its Fock builder.
                  (energy, occupied orbitals and energies), the two-electron
                  gradient and the full RHF gradient at that density.
   config_c3.npz  30-atom C/N/O/F/H, RHF/cc-pVDZ (300 bf): the same.
-  config_c5.npz  100-atom C/N/O/S/H, RHF/6-31+G* (1129 bf): core-Hamiltonian
-                 guess orbitals (float32; the density is 2 C C^T of their
-                 float64 values) and the oracle's J and K there as row sums,
+  config_c5.npz  100-atom C/N/O/S/H, RHF/6-31+G* (1129 bf): the oracle's J
+                 and K at a seeded bounded density (c5_density) as row sums,
                  Tr(DJ), Tr(DK) and 20000 seeded element samples.
-  c5x            adds to config_c5.npz the same quantities with the oracle's
-                 Rys roots in extended precision (oracle.set_root_precision):
-                 the reference's double-precision moment method carries
-                 relative root errors up to ~2e-11 at five roots, which this
-                 workload's 3.6e9 shell quartets turn into J/K deviations of
-                 ~1e-9 on elements of order 10; the extended reading shows
-                 which side of a device/oracle difference that error is on.
+  c5x            (optional) adds to config_c5.npz the same quantities with the
+                 oracle's Rys roots in extended precision
+                 (oracle.set_root_precision), a second reading that separates
+                 the reference's double-precision root error (up to ~2e-11
+                 relative at five roots) from a device-side difference.
 
 Usage: python tests/golden/make_config_fixtures.py [c2 c3 c5 c5x]   (about 2 h on 8 cores,
 c5x about 1 h more)
@@ -91,20 +88,23 @@ def scf_fixture(name, log):
                         c_occ=C, eps_occ=eps, grad_2e=g2, grad_rhf=g1 + g2, e_nuc=enuc)
 
 
+def c5_density(n, seed=5, scale=0.02):
+    """The C5 parity density: seeded, symmetric, elements of order `scale`.
+    (The core-Hamiltonian guess of this near-linearly-dependent 6-31+G* basis,
+    overlap eigenvalues down to 1.8e-8, has density elements up to 1e6: each
+    J element is then a cancellation of ~1e6-sized terms, and two FP64
+    evaluations of it differ by ~1e-9 whatever their quadrature.)"""
+    rng = np.random.default_rng(seed)
+    A = rng.normal(size=(n, n)) * scale
+    return A + A.T
+
+
 def c5_fixture(log):
     atoms, basis = workload("c5", 0)
     b = build_basis(atoms, basis)
     n = b.n_basis
     log("c5: %d atoms, %d bf" % (b.n_atoms, n))
-    S = oracle.one_electron(b, "S")
-    H = oracle.hcore(b)
-    w, U = np.linalg.eigh(S)
-    X = (U / np.sqrt(w)) @ U.T
-    _, Cp = np.linalg.eigh(X.T @ H @ X)
-    n_occ = b.n_electrons // 2
-    C32 = (X @ Cp)[:, :n_occ].astype(np.float32)
-    C = C32.astype(np.float64)
-    D = 2.0 * C @ C.T
+    D = c5_density(n)
     t0 = time.time()
     J, K, cnt = oracle.jk_direct(b, D)
     t_jk = time.time() - t0
@@ -113,12 +113,13 @@ def c5_fixture(log):
     rng = np.random.default_rng(5)
     idx = rng.integers(0, n, size=(20000, 2)).astype(np.int32)
     z, xyz = geometry(atoms)
-    meta = {"workload": "c5", "seed": 0, "basis": basis, "nbf": n, "n_occ": n_occ,
-            "density": "core-Hamiltonian guess: D = 2 C C^T, C = float64(c_occ_f32)",
+    meta = {"workload": "c5", "seed": 0, "basis": basis, "nbf": n,
+            "density": "c5_density(nbf): rng(5) normal(nbf, nbf) * 0.02, D = A + A^T",
+            "density_seed": 5, "density_scale": 0.02,
             "oracle_threads": oracle.max_threads(), "oracle_jk_s": t_jk,
             "shell_quartets": int(cnt[3]), "prim_quartets": int(cnt[2])}
     np.savez_compressed(os.path.join(HERE, "config_c5.npz"), meta=json.dumps(meta), z=z, xyz=xyz,
-                        c_occ_f32=C32, idx=idx, j_sample=J[idx[:, 0], idx[:, 1]], k_sample=K[idx[:, 0], idx[:, 1]],
+                        idx=idx, j_sample=J[idx[:, 0], idx[:, 1]], k_sample=K[idx[:, 0], idx[:, 1]],
                         j_rowsum=J.sum(1), k_rowsum=K.sum(1), tr_dj=float(np.sum(D * J)),
                         tr_dk=float(np.sum(D * K)))
 
@@ -129,8 +130,7 @@ def c5x_fixture(log):
     meta = json.loads(str(f["meta"]))
     atoms, basis = workload("c5", 0)
     b = build_basis(atoms, basis)
-    C = f["c_occ_f32"].astype(np.float64)
-    D = 2.0 * C @ C.T
+    D = c5_density(b.n_basis, int(meta["density_seed"]), float(meta["density_scale"]))
     idx = f["idx"]
     oracle.set_root_precision(True)
     try:
@@ -149,7 +149,7 @@ def c5x_fixture(log):
 
 
 def main():
-    which = sys.argv[1:] or ["c2", "c3", "c5", "c5x"]
+    which = sys.argv[1:] or ["c2", "c3", "c5"]
 
     def log(msg):
         print(msg, flush=True)
