@@ -249,6 +249,17 @@ int iqcp_batch_scf(iqcp_ctx* ctx, const iqcp_scf_options* opts, const double* D0
                    int* converged, int* iterations, double* D_out, double* grad);
 
 /*
+ * SAD initial density of one geometry (build_sad_density, scf/sad.rs:698-760):
+ * per element, a spherically averaged atomic RHF with fractional subshell
+ * occupations (PySCF AtomSphAverageRHF; sad.rs:207-640), the atomic blocks
+ * placed on the diagonal, zero between atoms.  D: nbf x nbf row-major (the
+ * matrix is symmetric).  The atomic integrals come from one-atom contexts on
+ * opts->device (NULL: default options).  Pack the densities of a batch in the
+ * iqcp_create_batch layout to start iqcp_batch_scf from them (D0).
+ */
+int iqcp_sad_density(const iqcp_basis_desc* basis, const iqcp_options* opts, double* D);
+
+/*
  * All unique ERIs in the reference's 8-fold compressed layout,
  * idx = P(P+1)/2 + Q, P = pair(i,j) >= Q = pair(k,l), pair(i,j) = i(i+1)/2 + j.
  * Replaces eri_compressed (integrals/eri/mod.rs:992-1070); out holds

@@ -123,6 +123,7 @@ EXPORTS = {
     "iqcp_scf_default_options": (None, [ctypes.POINTER(ScfOptions)]),
     "iqcp_batch_scf": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ScfOptions), _c_dbl_p, _c_dbl_p, _c_int_p,
                                       _c_int_p, _c_dbl_p, _c_dbl_p]),
+    "iqcp_sad_density": (ctypes.c_int, [ctypes.POINTER(_BasisDesc), ctypes.POINTER(_Options), _c_dbl_p]),
 }
 
 PAIR_CLASSES = ["ss", "ps", "pp", "ds", "dp", "dd"]
@@ -214,6 +215,20 @@ class BasisSet:
         """Plain arrays in the C ABI's shell layout (also used by the oracle)."""
         return (self.n_shells, self.l, self.nprim, self.atom_of_shell, self.center, self.exps, self.coefs,
                 self.n_atoms, self.xyz, self.z)
+
+    def sad_density(self, device=0):
+        """SAD initial density (iqcp_sad_density; build_sad_density, scf/sad.rs:698):
+        superposed spherically averaged atomic RHF densities, nbf x nbf."""
+        lib = load_library()
+        opts = _Options()
+        lib.iqcp_default_options(ctypes.byref(opts))
+        opts.device = device
+        D = np.empty((self.n_basis, self.n_basis))
+        desc = self._desc()
+        rc = lib.iqcp_sad_density(ctypes.byref(desc), ctypes.byref(opts), _dp(D))
+        if rc:
+            raise IqcpError(rc, "iqcp_sad_density")
+        return D
 
     def _desc(self):
         d = _BasisDesc()
@@ -465,6 +480,7 @@ class BatchFockEngine(FockEngine):
         opts.precision = precision
         opts.mixed_cutoff = mixed_cutoff
         opts.device = device
+        self.device = device
         n = len(self.bases)
         self._descs = (_BasisDesc * n)(*[b._desc() for b in self.bases])
         h = ctypes.c_void_p()

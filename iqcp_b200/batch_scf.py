@@ -53,9 +53,15 @@ class BatchRHF:
         eng._check(eng._lib.iqcp_batch_scf(eng._h, ctypes.byref(o), None, None, None, None, _dp(D), None))
         return D
 
+    def sad_guess(self):
+        """Packed SAD densities of every geometry (iqcp_sad_density per geometry;
+        the reference's guess for its optimiser and scan callers, scf/sad.rs:698)."""
+        return self.eng.pack([b.sad_density(self.eng.device) for b in self.bases])
+
     def run(self, e_tol=1e-9, d_tol=1e-7, err_tol=1e-5, max_iter=80, D0=None, gradients=True):
         """Iterate every geometry until all meet the three thresholds or max_iter;
-        D0: optional list of starting densities (default: core-Hamiltonian guess).
+        D0: optional starting densities, a list per geometry or a packed array
+        (sad_guess(); default: the core-Hamiltonian guess).
         With gradients, the RHF nuclear gradient at the final density comes back
         too (gradients())."""
         eng = self.eng
@@ -65,7 +71,9 @@ class BatchRHF:
         iters = ctypes.c_int(0)
         D = np.empty(eng.packed_size)
         g = np.zeros((eng.n_atoms, 3)) if gradients else None
-        d0 = eng.pack(D0) if D0 is not None else None
+        d0 = None
+        if D0 is not None:
+            d0 = np.ascontiguousarray(D0, dtype=np.float64) if np.ndim(D0) == 1 else eng.pack(D0)
         o = self._opts(e_tol, d_tol, err_tol, max_iter)
         eng._check(eng._lib.iqcp_batch_scf(eng._h, ctypes.byref(o), _dp(d0) if d0 is not None else None, _dp(E),
                                            conv.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), ctypes.byref(iters),
