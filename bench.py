@@ -352,7 +352,7 @@ def measure_batch(args):
             eng.set_precision(prec, MIXED_CUTOFF)
             torch.cuda.synchronize()
             t1 = time.perf_counter()
-            res = scf.run()
+            res = scf.run(D0=scf.sad_guess())     # SAD start, as the optimiser / scan callers (sad.rs:698)
             t2 = time.perf_counter()
             out.setdefault("scf", {})[name] = {
                 "iterations": res.iterations, "converged": int(res.converged.sum()), "seconds": t2 - t1,
@@ -379,7 +379,7 @@ def measure_batch(args):
                 out["scf"]["mixed"]["max_grad_error_vs_fp64_ha_bohr"] = float(
                     max(np.abs(g32s[i] - g64s[i]).max() for i in both))
         eng.set_precision(FP64)
-        out["scf"]["note"] = ("iqcp_batch_scf: RHF to dE 1e-9, rms dD 1e-7, DIIS error 1e-5 from the core guess, one "
+        out["scf"]["note"] = ("iqcp_batch_scf: RHF to dE 1e-9, rms dD 1e-7, DIIS error 1e-5 from the SAD guess (in the timed region), one "
                               "CUDA graph per iteration (Fock build, DIIS, purification), energy + RHF gradient "
                               "per geometry, wall time; converged geometries stop iterating.  Mixed against FP64 "
                               "after SCF compares two separately converged densities, which the DIIS threshold "
