@@ -337,6 +337,12 @@ constexpr int kTeamGradBudget = 2560;
 // (the fused phase A); up to 96 the spill is a few hundred bytes, which costs
 // less than the shared table it replaces.
 constexpr int kTeamFusedMaxTab = 96;
+// Register budget per thread of the gradient team kernel (sets its minimum
+// resident blocks): 128, i.e. 16 warps per SM where shared memory allows,
+// except for extended tables above 72 entries, whose register-resident fused
+// phase A then spills more than the extra warps gain ((dd|dp): 2.55 ms at 168
+// registers, 2.66 ms at 128; (dp|pp) 6.83 -> 6.67 ms, (dp|ds) 5.49 -> 5.01 ms)
+constexpr int team_grad_regs(int tsz) { return tsz <= 72 ? 128 : 168; }
 
 template <int LA, int LB, int LC, int LD>
 struct TeamGrad2 {
@@ -398,9 +404,10 @@ struct TeamGrad2 {
   static constexpr int CPL = (C::NCOMP + 31) / 32;
   static constexpr int WPB = team_warps_per_block(PER_WARP);
   // resident blocks per SM asked of the compiler: what shared memory allows,
-  // but no more than leaves 168 registers per thread (65536 / (MINB * 32 * WPB))
+  // but no more than leaves TREG registers per thread (65536 / (MINB * 32 * WPB))
+  static constexpr int TREG = team_grad_regs(TSZ);
   static constexpr int SMB = team_resident(WPB, PER_WARP) / WPB;
-  static constexpr int RGB = 65536 / (168 * 32 * WPB);
+  static constexpr int RGB = 65536 / (TREG * 32 * WPB);
   static constexpr int MINB = (SMB < RGB ? SMB : RGB) > 0 ? (SMB < RGB ? SMB : RGB) : 1;
   __host__ __device__ static constexpr int eidx(int a, int b, int c, int d) {
     return ((a * (EB + 1) + b) * (EC + 1) + c) * (ED + 1) + d;
