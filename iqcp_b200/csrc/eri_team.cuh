@@ -57,6 +57,13 @@ struct TeamJK {
                             C::NA * C::NC;
   static constexpr int PER_WARP = WORK + DB;
   static constexpr int CPL = (C::NCOMP + 31) / 32;
+  // resident 128-thread blocks asked of the compiler: 4 (128 registers, 16
+  // warps per SM) where shared memory admits them and the tables are small
+  // enough not to spill (<= 36 entries: ptxas 0-52 bytes); 1 otherwise (the
+  // 54- and 81-entry tables spill 250+ bytes at 128 registers)
+  static constexpr int SMEM_BLOCKS =
+      (228 * 1024) / (int(sizeof(double)) * (4 * PER_WARP + rys_tab_doubles<C::NR>()) + 1024);
+  static constexpr int MINB = C::TSZ <= 36 ? (SMEM_BLOCKS < 4 ? (SMEM_BLOCKS > 0 ? SMEM_BLOCKS : 1) : 4) : 1;
 };
 
 // One contracted quartet: phases A and B over all surviving primitive
@@ -112,7 +119,7 @@ __device__ __forceinline__ void team_prim_loop(const JKArgs& args, const ShellPa
 }
 
 template <typename R, int LA, int LB, int LC, int LD, bool DO_K>
-__global__ void __launch_bounds__(128) jk_team_kernel(JKArgs args) {
+__global__ void __launch_bounds__(128, TeamJK<LA, LB, LC, LD>::MINB) jk_team_kernel(JKArgs args) {
   using C = Cls<LA, LB, LC, LD>;
   using TM = TeamJK<LA, LB, LC, LD>;
   constexpr int NR = C::NR, TSZ = TM::TSP, CPL = TM::CPL;  // table stride
