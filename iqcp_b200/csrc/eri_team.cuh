@@ -384,7 +384,9 @@ struct TeamGrad2 {
   // the 40-atom 6-31G* step: batching gains 3-6% with pp and dd kets and
   // loses 15-40% with ds kets and for (dd|dp)
   static constexpr bool RBATCH = (LC == 1 && LD == 1) || (LC == 2 && LD == 2);
-  static constexpr int JCH = RBATCH ? 32 / NR : 1;
+  // at most 6 primitives: with 8, (dp|pp)'s four blocks of four warps (and
+  // the per-block gradient accumulator) exceed the SM's shared memory by 1.5 KB
+  static constexpr int JCH = RBATCH ? (32 / NR < 6 ? 32 / NR : 6) : 1;
   static constexpr int DBLK = C::NA * C::NB + C::NC * C::ND + C::NA * C::NC + C::NB * C::ND + C::NA * C::ND +
                               C::NB * C::NC;
   // shared footprint (doubles) with the tables of rch roots at a time
