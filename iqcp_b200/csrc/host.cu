@@ -91,6 +91,12 @@ struct iqcp_ctx {
   long long n_quartets = 0;
   double stats[4] = {0, 0, 0, 0};
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // class launches run concurrently on the context stream and these side
+  // streams (forked and joined with events), so one class's tail overlaps
+  // the next class's start
+  static constexpr int kSide = 3;
+  cudaStream_t side[kSide] = {nullptr, nullptr, nullptr};
+  cudaEvent_t fork_ev = nullptr, join_ev[kSide] = {nullptr, nullptr, nullptr};
   // per-launch timing of the quartet kernels (off unless requested)
   bool profile = false;
   std::vector<cudaEvent_t> pev;
@@ -341,7 +347,11 @@ bool capturing(const iqcp_ctx* ctx) {
 // Launch the quartet kernels of every non-empty class range; kind 0 = J/K,
 // 1 = gradient.  In a mixed call a class whose split flag is set launches
 // twice, pass 1 (FP64 share) then pass 2 (FP32 share); launch(r, pass,
-// counter) issues one launch.
+// counter, stream) issues one launch.  Launches go round-robin to the context
+// stream and the side streams, forked after the counters' reset and joined
+// before the end event: each launch has its own work counter and every
+// kernel adds its results atomically, so they may overlap (a persistent
+// kernel's blocks start on the SMs that the previous one's tail frees).
 template <typename F>
 int run_ranges(iqcp_ctx* ctx, int kind, F&& launch) {
   ctx->in_capture = capturing(ctx);
@@ -354,6 +364,17 @@ int run_ranges(iqcp_ctx* ctx, int kind, F&& launch) {
   ctx->launch_log.clear();
   CK(cudaMemsetAsync(ctx->d_counters + 2 * kind * nr, 0, sizeof(int) * 2 * nr, ctx->stream));
   if (!ctx->in_capture) CK(cudaEventRecord(ctx->ev0, ctx->stream));
+  // with per-launch profiling on, the launches stay on the context stream so
+  // that each launch's events time it alone
+  const int nst = prof ? 1 : 1 + iqcp_ctx::kSide;
+  cudaStream_t streams[1 + iqcp_ctx::kSide] = {ctx->stream};
+  if (nst > 1) {
+    CK(cudaEventRecord(ctx->fork_ev, ctx->stream));
+    for (int s = 0; s < iqcp_ctx::kSide; ++s) {
+      streams[1 + s] = ctx->side[s];
+      CK(cudaStreamWaitEvent(ctx->side[s], ctx->fork_ev, 0));
+    }
+  }
   int launches = 0;
   for (size_t i = 0; i < nr; ++i) {
     const TaskRange& r = ctx->ranges[i];
@@ -362,12 +383,17 @@ int run_ranges(iqcp_ctx* ctx, int kind, F&& launch) {
     for (int ps = 0; ps < (split ? 2 : 1); ++ps) {
       const int pass = split ? ps + 1 : 0;
       const int ev = int(2 * (2 * i + ps));
-      if (prof) CK(cudaEventRecord(ctx->pev[ev], ctx->stream));
-      CK(launch(r, pass, ctx->d_counters + (2 * kind + ps) * nr + i));
-      if (prof) CK(cudaEventRecord(ctx->pev[ev + 1], ctx->stream));
+      cudaStream_t st = streams[launches % nst];
+      if (prof) CK(cudaEventRecord(ctx->pev[ev], st));
+      CK(launch(r, pass, ctx->d_counters + (2 * kind + ps) * nr + i, st));
+      if (prof) CK(cudaEventRecord(ctx->pev[ev + 1], st));
       ++launches;
       ctx->launch_log.push_back({kind + (pass == 2 ? 2 : 0), r.X, r.Y, 0.f, pass == 2 ? 0 : r.quartets, ev});
     }
+  }
+  for (int s = 0; nst > 1 && s < iqcp_ctx::kSide; ++s) {
+    CK(cudaEventRecord(ctx->join_ev[s], ctx->side[s]));
+    CK(cudaStreamWaitEvent(ctx->stream, ctx->join_ev[s], 0));
   }
   if (!ctx->in_capture) CK(cudaEventRecord(ctx->ev1, ctx->stream));
   ctx->stats[0] = (double)ctx->n_quartets;
@@ -387,10 +413,10 @@ int run_jk_device(iqcp_ctx* ctx, const double* dD, bool want_k) {
   }
   CK(cudaMemsetAsync(ctx->d_Jt, 0, bytes, ctx->stream));
   if (want_k) CK(cudaMemsetAsync(ctx->d_Kt, 0, bytes, ctx->stream));
-  return run_ranges(ctx, 0, [&](const TaskRange& r, int pass, int* counter) {
+  return run_ranges(ctx, 0, [&](const TaskRange& r, int pass, int* counter, cudaStream_t st) {
     const JKArgs a = jk_args(ctx, r, ctx->d_Ds, ctx->d_Jt, want_k ? ctx->d_Kt : nullptr,
                              pass == 2 ? r.mode32[0] : r.mode[0], pass, counter);
-    return launch_jk(r.X, r.Y, a, ctx->stream);
+    return launch_jk(r.X, r.Y, a, st);
   });
 }
 
@@ -500,6 +526,11 @@ static int create_batch(int nmol, const iqcp_basis_desc* descs, const iqcp_optio
   ctx->stream = ctx->own_stream;
   CK(cudaEventCreate(&ctx->ev0));
   CK(cudaEventCreate(&ctx->ev1));
+  CK(cudaEventCreateWithFlags(&ctx->fork_ev, cudaEventDisableTiming));
+  for (int s = 0; s < iqcp_ctx::kSide; ++s) {
+    CK(cudaStreamCreateWithFlags(&ctx->side[s], cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&ctx->join_ev[s], cudaEventDisableTiming));
+  }
   ctx->n_mol = nmol;
   const double kthr = ctx->opt.prim_threshold;
 
@@ -745,6 +776,11 @@ void iqcp_destroy(iqcp_ctx* ctx) {
   cudaFree(ctx->d_sph_info);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+  if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
+  for (int s = 0; s < iqcp_ctx::kSide; ++s) {
+    if (ctx->join_ev[s]) cudaEventDestroy(ctx->join_ev[s]);
+    if (ctx->side[s]) cudaStreamDestroy(ctx->side[s]);
+  }
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
   delete ctx;
 }
@@ -862,10 +898,10 @@ int iqcp_jk_device_noalloc(iqcp_ctx* ctx, const double* dD, double* dJ, double* 
   }
   CK(cudaMemsetAsync(Jt, 0, sizeof(double) * nn, ctx->stream));
   if (want_k) CK(cudaMemsetAsync(Kt, 0, sizeof(double) * nn, ctx->stream));
-  rc = run_ranges(ctx, 0, [&](const TaskRange& r, int pass, int* counter) {
+  rc = run_ranges(ctx, 0, [&](const TaskRange& r, int pass, int* counter, cudaStream_t st) {
     const JKArgs a = jk_args(ctx, r, Ds, Jt, want_k ? Kt : nullptr, pass == 2 ? r.mode32[0] : r.mode[0], pass,
                              counter);
-    return launch_jk(r.X, r.Y, a, ctx->stream);
+    return launch_jk(r.X, r.Y, a, st);
   });
   if (rc) return rc;
   CK(launch_symmetrize(Jt, ctx->d_ang, ctx->pack, dJ, ctx->stream));
@@ -935,11 +971,11 @@ int iqcp_jk_multi_device(iqcp_ctx* ctx, int nset, const double* dD, double* dJ, 
   ctx->mixed_call = false;  // response densities: FP64 quadrature
   CK(cudaMemsetAsync(Jt, 0, sizeof(double) * nn * nset, ctx->stream));
   if (want_k) CK(cudaMemsetAsync(Kt, 0, sizeof(double) * nn * nset, ctx->stream));
-  rc = run_ranges(ctx, 0, [&](const TaskRange& r, int pass, int* counter) {
+  rc = run_ranges(ctx, 0, [&](const TaskRange& r, int pass, int* counter, cudaStream_t st) {
     JKArgs a = jk_args(ctx, r, Ds, Jt, want_k ? Kt : nullptr, r.mode[0], pass, counter);
     a.nset = nset;
     a.set_stride = nn;
-    return launch_jk(r.X, r.Y, a, ctx->stream);
+    return launch_jk(r.X, r.Y, a, st);
   });
   if (rc) return rc;
   for (int s = 0; s < nset; ++s) {
@@ -1124,10 +1160,10 @@ int iqcp_eri_grad_device(iqcp_ctx* ctx, const double* dD, double hf_frac, double
     rc = prepare_mixed(ctx, dD, 1);
     if (rc) return rc;
   }
-  rc = run_ranges(ctx, 1, [&](const TaskRange& r, int pass, int* counter) {
+  rc = run_ranges(ctx, 1, [&](const TaskRange& r, int pass, int* counter, cudaStream_t st) {
     const GradArgs a = grad_args(ctx, r, ctx->d_Ds, 0.25 * hf_frac, dgrad, pass == 2 ? r.mode32[1] : r.mode[1],
                                  pass, counter);
-    return launch_grad(r.X, r.Y, a, ctx->stream);
+    return launch_grad(r.X, r.Y, a, st);
   });
   if (rc) return rc;
   return finish_stats(ctx);
