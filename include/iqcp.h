@@ -122,7 +122,11 @@ int iqcp_set_precision(iqcp_ctx* ctx, int precision, double mixed_cutoff);
  * Run the context's work on this CUDA stream (cudaStream_t); NULL = the
  * context's own stream, which is created non-blocking (it does not order with
  * the legacy default stream).  A caller working on the legacy default stream
- * passes cudaStreamLegacy, not NULL.
+ * passes cudaStreamLegacy, not NULL.  Inside a J/K build or gradient the
+ * class kernels also run on three side streams of the context, forked from
+ * this stream by an event and joined back to it before the call's last
+ * operation, so work queued on this stream before the call precedes all of
+ * them and work queued after it follows all of them (in stream capture too).
  */
 int iqcp_set_stream(iqcp_ctx* ctx, void* stream);
 
